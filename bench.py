@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of CURFIL's random-forest training hot path on B200.
+
+Workload (the plain-method full-size configuration): 200 seeded synthetic RGB-D frames 640x480
+(40 Voronoi cells, 40 classes, uint8 colour, uint16 depth with 10% holes), 4000 samples per image
+(class-uniform, divided over the trees as RandomForestImage::train does), 3 trees to depth 20,
+2000 candidate features x 20 thresholds per level, minSampleCount 50, offsets <= 60, boxes <= 15.
+
+A step trains the forest's trees level-batched from their sample lists on the resident dataset
+(integral images 1.2 GB, larger than L2). Metric: feature evaluations per second (one evaluation =
+one (sample, candidate feature) response compared against all thresholds and binned).
+`e2e` trains through cf_forest_train from host frames (upload, integral images, host sampling,
+training, tree download). Prediction of 50 frames with the trained forest is reported beside it.
+Under torchrun every rank trains its own trees (trees are independent; no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = dict(images=200, width=640, height=480, cells=40, classes=40, samples_per_image=4000, trees=3, max_depth=20,
+         features=2000, thresholds=20, min_samples=50, box_radius=60, region_size=15, predict_images=50, seed=2026)
+BYTES_DEPTH_EVAL = 64   # 2 boxes x 4 corners x (int32 depth sum + int32 valid count)
+BYTES_COLOR_EVAL = 32   # 2 boxes x 4 corners x float32
+METRIC = "train feature-evals/s"
+
+
+def workload_config():
+    return {"workload": "plain method full size: %d RGB-D frames %dx%d, %d classes, %d samples/image, %d trees "
+                        "depth %d, %d features x %d thresholds, minSampleCount %d" % (
+                            W["images"], W["width"], W["height"], W["classes"], W["samples_per_image"], W["trees"],
+                            W["max_depth"], W["features"], W["thresholds"], W["min_samples"]),
+            "images": W["images"], "frame": "%dx%d" % (W["width"], W["height"]), "classes": W["classes"],
+            "trees_per_gpu": W["trees"], "max_depth": W["max_depth"], "features": W["features"],
+            "thresholds": W["thresholds"], "samples_per_image": W["samples_per_image"],
+            "l2": "inputs larger than L2 (integral images 1.23 GB)"}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_data():
+    import curfil_b200 as cf
+    return cf.synthetic_frames(W["seed"], W["images"], W["width"], W["height"], W["cells"], W["classes"])
+
+
+def train_config():
+    import curfil_b200 as cf
+    return cf.TrainConfig(random_seed=4711, samples_per_image=W["samples_per_image"], feature_count=W["features"],
+                          min_sample_count=W["min_samples"], max_depth=W["max_depth"], box_radius=W["box_radius"],
+                          region_size=W["region_size"], thresholds=W["thresholds"])
+
+
+def tree_samples(labels, depth, cfg, tree_ids):
+    import curfil_b200 as cf
+    seed = cf.forest_seed(cfg.random_seed)
+    out = []
+    for t in tree_ids:
+        s, prior, counter = cf.sample_tree_pixels(labels, depth, W["classes"], cfg, W["trees"], seed + t)
+        out.append((t, s, prior, counter))
+    return out
+
+
+# ----------------------------------------------------------------------------------------- CPU baseline
+def cpu_root_split_search(rgb, depth, labels, seconds=15.0, threads=None):
+    """The reference's CPU split search (FeatureEvaluationCPU + calculateScores + argmax) on the oracle,
+    for the root node of tree 0 with as many candidate features as fit in ~`seconds`."""
+    import curfil_b200 as cf
+    from oracle import pyoracle as orc
+    threads = threads or os.cpu_count()
+    cfg = train_config()
+    (_, samples, _, counter), = tree_samples(labels, depth, cfg, [0])
+    ods = orc.integral(rgb, depth)
+    s = samples.view(orc.SAMPLE_DTYPE)
+    feats, thr = orc.generate_features(ods, s, 12345, W["features"], W["thresholds"], W["box_radius"],
+                                       W["region_size"])
+    hist = np.bincount(s["label"], minlength=W["classes"]).astype(np.uint32)
+
+    def run(F):
+        idx = np.linspace(0, W["features"] - 1, F).astype(int)   # keep the depth/colour mix
+        f, t = np.ascontiguousarray(feats[:, idx]), np.ascontiguousarray(thr[:, idx])
+        t0 = time.perf_counter()
+        counters = orc.histograms(ods, s, f, t, W["classes"], threads=threads)
+        sc = orc.scores(counters, hist)
+        orc.best_split(sc)
+        return time.perf_counter() - t0
+
+    probe_f = 8
+    dt = run(probe_f)
+    F = int(max(probe_f, min(W["features"], probe_f * seconds / max(dt, 1e-6))))
+    F = max(2, F - F % 2)
+    dt = run(F)
+    evals = len(s) * F
+    return {"value": evals / dt, "unit": "feature-evals/s", "cores": threads, "kind": "port",
+            "sample": "root-node split search of tree 0: %d samples x %d of %d candidate features x %d thresholds "
+                      "(oracle restatement of FeatureEvaluationCPU + calculateScores, OpenMP)" % (
+                          len(s), F, W["features"], W["thresholds"]),
+            "seconds": dt}, ods
+
+
+# ----------------------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import curfil_b200 as cf  # noqa: F401  (synthetic frames only)
+    rgb, depth, labels = make_data()
+    budget = max(5.0, 60.0 / max(1, args.steps + args.warmup))
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        base, _ = cpu_root_split_search(rgb, depth, labels, seconds=budget)
+        if i >= args.warmup:
+            vals.append(base["value"])
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": "feature-evals/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": base["seconds"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": workload_config(),
+            "cpu_baseline": {"value": value, "unit": "feature-evals/s", "cores": base["cores"], "kind": "port",
+                             "sample": base["sample"]},
+            "e2e": {"value": value, "unit": "feature-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference cannot be built here (Boost, TBB, Vigra, cuv::ndarray absent; texture references "
+                    "removed in CUDA 12); its CPU path is timed through the oracle restatement"}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------- our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import curfil_b200 as cf
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    rgb, depth, labels = make_data()
+    cfg = train_config()
+    ctx = cf.Context(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    ds = cf.Dataset.from_raw(ctx, rgb, depth)
+    tree_ids = [rank * W["trees"] + t for t in range(W["trees"])]
+    per_tree = tree_samples(labels, depth, cfg, tree_ids)
+
+    def step():
+        trees, evals = [], 0
+        for t, s, prior, counter in per_tree:
+            tree, _ = cf.train_tree(ds, s, W["classes"], cfg, tree_id=t, seed_counter=counter)
+            tree.set_prior(prior)
+            evals += tree.train_stats()[0]
+            trees.append(tree)
+        return trees, evals
+
+    for _ in range(args.warmup):
+        trees, evals_per_step = step()
+    torch.cuda.synchronize()
+    barrier()
+    ctx.reset_timing()
+    ctx.set_timing(True)
+    launches0 = ctx.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier()
+        start.record(stream)
+        total_evals = 0
+        for _ in range(args.steps):
+            trees, ev = step()
+            total_evals += ev
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ctx.set_timing(False)
+    launches = ctx.launch_count() - launches0
+    ms = start.elapsed_time(end)
+    ms_max = max_over_ranks(ms)
+    all_evals = sum_over_ranks(total_evals)
+    value = all_evals / (ms_max / 1e3)
+    eval_ms, eval_launches = ctx.kernel_time("level_eval")
+    kernel_ms = {k: ctx.kernel_time(k)[0] for k in ("level_eval", "gen_features", "route_flags", "route_scatter",
+                                                     "scan", "reduce_candidates", "sort_features")}
+
+    # algorithmic bytes of the level-batched evaluation: half the candidates are depth features
+    bytes_per_eval = (BYTES_DEPTH_EVAL + BYTES_COLOR_EVAL) / 2.0
+    achieved = total_evals * bytes_per_eval / (eval_ms / 1e3) / 1e9 if eval_ms > 0 else None
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "level_eval_traffic.txt")
+    if os.path.exists(tp):
+        for ln in open(tp):
+            if ln.startswith("dram_bytes_per_feature_eval:"):
+                traffic = float(ln.split(":")[1]) * total_evals / max(1, eval_launches)
+
+    # prediction of 50 resident frames with the trained forest
+    forest = cf.Forest(ctx, trees)
+    n_pred = W["predict_images"]
+    probs = torch.empty((n_pred, W["classes"], W["height"], W["width"]), dtype=torch.float32, device=local)
+    lab = torch.empty((n_pred, W["height"], W["width"]), dtype=torch.uint8, device=local)
+    with torch.cuda.stream(stream):
+        forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
+        pstart, pend = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        pstart.record(stream)
+        reps = 3
+        for _ in range(reps):
+            forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
+        pend.record(stream)
+        torch.cuda.synchronize()
+    pred_ms = pstart.elapsed_time(pend) / reps
+    mpx = n_pred * W["width"] * W["height"] / (pred_ms / 1e3) / 1e6
+    forest.close()
+
+    # end to end through cf_forest_train with host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        t0 = time.perf_counter()
+        e2e_evals = 0
+        d2h = 0
+        for _ in range(args.e2e_steps):
+            ts = cf.train_forest(ctx, rgb, depth, labels, W["classes"], cfg, W["trees"])
+            for t in ts:
+                e2e_evals += t.train_stats()[0]
+                d2h += t.num_nodes * (4 * 4 + 11 + 4 + 8 + 4 * W["classes"])
+        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(e2e_s)
+        e2e = {"value": sum_over_ranks(e2e_evals) / e2e_s, "unit": "feature-evals/s",
+               "h2d_bytes_per_step": int(rgb.nbytes + depth.nbytes),
+               "d2h_bytes_per_step": int(d2h / args.e2e_steps),
+               "note": "cf_forest_train: upload, GPU integral images, host class-uniform sampling (one thread, "
+                       "as the reference's reproducible mode), level-batched training, tree download"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = cpu_root_split_search(rgb, depth, labels, seconds=15.0)
+        cpu.pop("seconds", None)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "feature-evals/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(workload_config(), parallelism="trees sharded over %d GPU(s)" % world),
+                "roofline": {"bound": "hbm", "kernel": "level_eval", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                             "peak_source": peak_kind, "bytes_per_eval": bytes_per_eval,
+                             "avg_launch_ms": eval_ms / max(1, eval_launches), "launches": eval_launches},
+                "kernel_ms": kernel_ms,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks.summary(),
+                "predict": {"images": n_pred, "mpx_per_s": mpx, "ms_per_batch": pred_ms,
+                            "ms_per_frame": pred_ms / n_pred, "trees": W["trees"]},
+                "feature_evals_per_step": total_evals / args.steps}
+        print(json.dumps(line), flush=True)
+    ds.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,356 @@
+// Dense per-pixel forest prediction (kernel e).
+//
+// Replaces classifyKernel + normalizeProbabilitiesKernel + maxProbabilitiesKernel
+// (random_tree_image_gpu.cu:1237-1453), launched once per tree per image in the reference, by one
+// launch over all trees and all frames of a batch (frames may differ in size). One thread per
+// pixel: its depth comes from the integral image as on the reference's CPU path
+// (random_tree_image.h:140-165); each tree is walked with the exact double feature response,
+// NaN going right; the leaf histograms are summed in registers, normalised by their double sum
+// and arg-maxed with the lowest label winning ties (random_forest_image.cpp:307-345). The top
+// levels of every tree are staged in shared memory, the rest is read through L1/L2.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "features.h"
+#include "forest.h"
+
+namespace cf {
+
+namespace {
+
+constexpr int kClassifyThreads = 256;
+constexpr int kSmemNodesBudget = 2048;  // 32 KB of cached nodes per CTA
+
+__device__ __forceinline__ float pixel_depth(const int2* D, int W, int x, int y) {
+    const int2 c = __ldg(D + static_cast<long long>(y) * W + x);
+    const int2 a = y > 0 ? __ldg(D + static_cast<long long>(y - 1) * W + x) : make_int2(0, 0);
+    const int2 l = x > 0 ? __ldg(D + static_cast<long long>(y) * W + x - 1) : make_int2(0, 0);
+    const int2 al = (x > 0 && y > 0) ? __ldg(D + static_cast<long long>(y - 1) * W + x - 1) : make_int2(0, 0);
+    const int valid = c.y - (l.y + a.y - al.y);
+    if (valid != 1) return 0.0f;
+    const int mm = static_cast<int>(static_cast<uint32_t>(c.x) -
+                                    (static_cast<uint32_t>(l.x) + static_cast<uint32_t>(a.x) - static_cast<uint32_t>(al.x)));
+    if (mm <= 0) return 0.0f;
+    return __fdiv_rn(static_cast<float>(mm), 1000.0f);
+}
+
+template <int CMAX>
+__global__ void __launch_bounds__(kClassifyThreads)
+classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tree_base, int num_trees, int cache,
+                const float* __restrict__ leaves, int C, const FrameDesc* __restrict__ frames, int num_frames) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    PackedNode* s_nodes = reinterpret_cast<PackedNode*>(smem);
+    // which frame does this CTA serve
+    int lo = 0, hi = num_frames - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (frames[mid].first_block <= static_cast<int>(blockIdx.x)) lo = mid; else hi = mid - 1;
+    }
+    const FrameDesc fr = frames[lo];
+    // stage the top `cache` nodes of every tree
+    for (int i = threadIdx.x; i < num_trees * cache; i += blockDim.x) {
+        const int t = i / cache, k = i - t * cache;
+        const int nt = tree_base[t + 1] - tree_base[t];
+        if (k < nt) s_nodes[i] = nodes[tree_base[t] + k];
+    }
+    __syncthreads();
+    const long long plane = static_cast<long long>(fr.width) * fr.height;
+    const long long p = static_cast<long long>(blockIdx.x - fr.first_block) * blockDim.x + threadIdx.x;
+    if (p >= plane) return;
+    const int y = static_cast<int>(p / fr.width);
+    const int x = static_cast<int>(p - static_cast<long long>(y) * fr.width);
+    DsView ds;
+    ds.color = fr.color;
+    ds.depth = fr.depth;
+    ds.n = 1;
+    ds.width = fr.width;
+    ds.height = fr.height;
+    ds.plane = plane;
+    const float depth = pixel_depth(fr.depth, fr.width, x, y);
+
+    float acc[CMAX];
+#pragma unroll
+    for (int c = 0; c < CMAX; c++) acc[c] = 0.0f;
+    for (int t = 0; t < num_trees; t++) {
+        const int base = tree_base[t];
+        const int nt = tree_base[t + 1] - base;
+        const int cached = min(cache, nt);
+        int idx = 0;
+        uint32_t meta;
+        for (;;) {
+            PackedNode nd;
+            if (idx < cached) nd = s_nodes[t * cache + idx];
+            else nd = nodes[base + idx];
+            meta = nd.meta;
+            if (meta & 0x80000000u) break;
+            FeatParams fp;
+            fp.o1x = nd.o1x;
+            fp.o1y = nd.o1y;
+            fp.o2x = nd.o2x;
+            fp.o2y = nd.o2y;
+            fp.r1x = nd.r1x;
+            fp.r1y = nd.r1y;
+            fp.r2x = nd.r2x;
+            fp.r2y = nd.r2y;
+            fp.type = static_cast<uint8_t>((meta >> 26) & 1u);
+            fp.ch1 = static_cast<uint8_t>((meta >> 27) & 3u);
+            fp.ch2 = static_cast<uint8_t>((meta >> 29) & 3u);
+            const double r = feature_response(ds, 0, x, y, depth, fp, false);
+            idx = static_cast<int>(meta & 0x03FFFFFFu) + ((r <= static_cast<double>(nd.threshold)) ? 0 : 1);
+        }
+        const float* row = leaves + static_cast<long long>(meta & 0x7FFFFFFFu) * C;
+#pragma unroll
+        for (int c = 0; c < CMAX; c++)
+            if (c < C) acc[c] = __fadd_rn(acc[c], __ldg(row + c));
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int c = 0; c < CMAX; c++)
+        if (c < C) sum = __dadd_rn(sum, static_cast<double>(acc[c]));
+    float best = -1.0f;
+    int label = 0;
+#pragma unroll
+    for (int c = 0; c < CMAX; c++) {
+        if (c < C) {
+            const float v = __double2float_rn(__ddiv_rn(static_cast<double>(acc[c]), sum));
+            if (fr.probs) fr.probs[c * plane + p] = v;
+            if (v > best) {
+                best = v;
+                label = c;
+            }
+        }
+    }
+    if (fr.labels) fr.labels[p] = static_cast<uint8_t>(label);
+}
+
+template <int CMAX>
+void launch_classify(cf_context* ctx, cudaStream_t stream, const cf_forest* f, const FrameDesc* frames, int num_frames,
+                     int blocks) {
+    const size_t smem = sizeof(PackedNode) * f->num_trees * f->cache_per_tree;
+    CF_CUDA_CHECK(cudaFuncSetAttribute(classify_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(std::max<size_t>(smem, 1))));
+    launch_on(ctx, stream, "classify", dim3(blocks), dim3(kClassifyThreads), smem, classify_kernel<CMAX>, f->nodes.get(),
+           f->d_tree_base.get(), f->num_trees, f->cache_per_tree, f->leaves.get(), f->C, frames, num_frames);
+}
+
+}  // namespace
+
+int classify_blocks_for(int width, int height) {
+    const long long plane = static_cast<long long>(width) * height;
+    return static_cast<int>((plane + kClassifyThreads - 1) / kClassifyThreads);
+}
+
+void classify_frames(cf_context* ctx, const cf_forest* forest, const FrameDesc* frames_dev, int num_frames,
+                     int total_blocks, cudaStream_t stream) {
+    if (stream == nullptr) stream = ctx->stream;
+    const int C = forest->C;
+    if (C <= 8) launch_classify<8>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+    else if (C <= 16) launch_classify<16>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+    else if (C <= 32) launch_classify<32>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+    else if (C <= 40) launch_classify<40>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+    else if (C <= 64) launch_classify<64>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+    else if (C <= 128) launch_classify<128>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+    else launch_classify<256>(ctx, stream, forest, frames_dev, num_frames, total_blocks);
+}
+
+// detail::normalizeHistogram (random_tree.cpp:54-104)
+void normalize_histogram(int C, const uint32_t* h, const uint32_t* prior, double bias, bool use_prior, double* out) {
+    std::vector<double> w(C);
+    double psum = 0;
+    for (int i = 0; i < C; i++) psum += prior[i];
+    for (int i = 0; i < C; i++) w[i] = prior[i] / psum;
+    double sum = 0;
+    for (int i = 0; i < C; i++) sum += h[i];
+    for (int i = 0; i < C; i++) {
+        out[i] = h[i] - bias * sum;
+        if (out[i] < 0.0) out[i] = 0.0;
+    }
+    sum = 0;
+    for (int i = 0; i < C; i++) sum += out[i];
+    if (sum > 0)
+        for (int i = 0; i < C; i++) out[i] = use_prior ? out[i] / sum * w[i] : out[i] / sum;
+}
+
+}  // namespace cf
+
+using namespace cf;
+
+namespace {
+
+void predict_frames(cf_forest* f, std::vector<FrameDesc>& frames) {
+    cf_context* ctx = f->ctx;
+    int blocks = 0;
+    for (auto& fr : frames) {
+        fr.first_block = blocks;
+        blocks += classify_blocks_for(fr.width, fr.height);
+    }
+    f->frames.reserve(frames.size());
+    CF_CUDA_CHECK(cudaMemcpyAsync(f->frames.get(), frames.data(), sizeof(FrameDesc) * frames.size(),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    classify_frames(ctx, f, f->frames.get(), static_cast<int>(frames.size()), blocks);
+}
+
+}  // namespace
+
+extern "C" {
+
+cf_status cf_forest_create(cf_context* ctx, int num_trees, cf_tree* const* trees, const uint32_t* prior,
+                           double histogram_bias, int use_labels_prior, cf_forest** out) {
+    return guard([&] {
+        CF_REQUIRE(ctx && trees && out, "cf_forest_create: NULL argument");
+        CF_REQUIRE(num_trees >= 1, "cannot construct empty forest");
+        make_current(ctx);
+        const int C = trees[0]->C;
+        for (int t = 0; t < num_trees; t++) {
+            CF_REQUIRE(trees[t] != nullptr, "cf_forest_create: NULL tree");
+            CF_REQUIRE(trees[t]->C == C, "different number of classes in trees");
+            CF_REQUIRE(prior != nullptr || static_cast<int>(trees[t]->prior.size()) == C,
+                       "cf_forest_create: no class prior given and the tree carries none");
+        }
+        auto* f = new cf_forest();
+        std::unique_ptr<cf_forest> guard_f(f);
+        f->ctx = ctx;
+        f->num_trees = num_trees;
+        f->C = C;
+        std::vector<PackedNode> packed;
+        std::vector<float> leaves;
+        std::vector<int> base(num_trees + 1, 0);
+        std::vector<double> norm(C);
+        for (int t = 0; t < num_trees; t++) {
+            const cf_tree* tr = trees[t];
+            base[t] = static_cast<int>(packed.size());
+            CF_REQUIRE(tr->num_nodes < (1 << 26), "tree too large for the packed node format");
+            const uint32_t* pr = prior ? prior : tr->prior.data();
+            for (int i = 0; i < tr->num_nodes; i++) {
+                PackedNode pn;
+                const int8_t* fe = &tr->feature[static_cast<size_t>(i) * 11];
+                pn.o1x = fe[1];
+                pn.o1y = fe[2];
+                pn.o2x = fe[3];
+                pn.o2y = fe[4];
+                pn.r1x = fe[5];
+                pn.r1y = fe[6];
+                pn.r2x = fe[7];
+                pn.r2y = fe[8];
+                if (tr->left[i] < 0) {
+                    normalize_histogram(C, &tr->hist[static_cast<size_t>(i) * C], pr, histogram_bias,
+                                        use_labels_prior != 0, norm.data());
+                    const int64_t row = static_cast<int64_t>(leaves.size() / C);
+                    CF_REQUIRE(row < 0x7FFFFFFF, "too many leaves");
+                    for (int c = 0; c < C; c++) leaves.push_back(static_cast<float>(norm[c]));
+                    pn.threshold = std::nanf("");
+                    pn.meta = 0x80000000u | static_cast<uint32_t>(row);
+                } else {
+                    CF_REQUIRE(tr->left[i] > i && tr->left[i] + 1 < tr->num_nodes, "corrupt tree: bad child index");
+                    pn.threshold = tr->threshold[i];
+                    pn.meta = static_cast<uint32_t>(tr->left[i]) | (static_cast<uint32_t>(fe[0] & 1) << 26) |
+                              (static_cast<uint32_t>(fe[9] & 3) << 27) | (static_cast<uint32_t>(fe[10] & 3) << 29);
+                }
+                packed.push_back(pn);
+            }
+        }
+        base[num_trees] = static_cast<int>(packed.size());
+        f->tree_base = base;
+        f->num_nodes = static_cast<int64_t>(packed.size());
+        f->num_leaves = static_cast<int64_t>(leaves.size() / C);
+        f->cache_per_tree = std::max(1, kSmemNodesBudget / num_trees);
+        f->nodes.reserve(packed.size());
+        f->d_tree_base.reserve(base.size());
+        f->leaves.reserve(leaves.size());
+        CF_CUDA_CHECK(cudaMemcpyAsync(f->nodes.get(), packed.data(), sizeof(PackedNode) * packed.size(),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(f->d_tree_base.get(), base.data(), sizeof(int) * base.size(),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(f->leaves.get(), leaves.data(), sizeof(float) * leaves.size(),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+        *out = guard_f.release();
+    });
+}
+
+cf_status cf_forest_destroy(cf_forest* forest) {
+    return guard([&] {
+        if (!forest) return;
+        cudaSetDevice(forest->ctx->device);
+        cudaStreamSynchronize(forest->ctx->stream);
+        delete forest;
+    });
+}
+
+cf_status cf_forest_info(cf_forest* forest, int* num_trees, int* num_classes, int64_t* num_nodes) {
+    return guard([&] {
+        CF_REQUIRE(forest, "cf_forest_info: forest is NULL");
+        if (num_trees) *num_trees = forest->num_trees;
+        if (num_classes) *num_classes = forest->C;
+        if (num_nodes) *num_nodes = forest->num_nodes;
+    });
+}
+
+cf_status cf_predict_dataset(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
+                             uint8_t* labels) {
+    return guard([&] {
+        CF_REQUIRE(forest && ds, "cf_predict_dataset: NULL argument");
+        CF_REQUIRE(first >= 0 && count >= 1 && first + count <= ds->n, "cf_predict_dataset: image range");
+        CF_REQUIRE(ds->ctx == forest->ctx, "cf_predict_dataset: dataset and forest belong to different contexts");
+        make_current(forest->ctx);
+        const long long plane = static_cast<long long>(ds->width) * ds->height;
+        std::vector<FrameDesc>& frames = forest->h_frames;
+        frames.resize(count);
+        for (int i = 0; i < count; i++) {
+            FrameDesc& fr = frames[i];
+            fr.color = ds->color.get() + (first + i) * plane * 3;
+            fr.depth = ds->depth.get() + (first + i) * plane;
+            fr.probs = probabilities ? probabilities + static_cast<long long>(i) * forest->C * plane : nullptr;
+            fr.labels = labels ? labels + static_cast<long long>(i) * plane : nullptr;
+            fr.width = ds->width;
+            fr.height = ds->height;
+            fr.pad = 0;
+        }
+        predict_frames(forest, frames);
+    });
+}
+
+cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, const uint8_t* rgb,
+                          const uint16_t* depth_mm, float* probabilities, uint8_t* labels) {
+    return guard([&] {
+        CF_REQUIRE(forest && rgb && depth_mm, "cf_predict_host: NULL argument");
+        CF_REQUIRE(count >= 1 && width >= 1 && height >= 1, "cf_predict_host: empty input");
+        cf_context* ctx = forest->ctx;
+        make_current(ctx);
+        const size_t plane = static_cast<size_t>(width) * height;
+        forest->raw_rgb.reserve(plane * 3 * count);
+        forest->raw_depth.reserve(plane * count);
+        forest->color.reserve(plane * 3 * count);
+        forest->depth.reserve(plane * count);
+        if (probabilities) forest->probs.reserve(plane * forest->C * count);
+        forest->labels.reserve(plane * count);
+        CF_CUDA_CHECK(cudaMemcpyAsync(forest->raw_rgb.get(), rgb, plane * 3 * count, cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(forest->raw_depth.get(), depth_mm, plane * 2 * count, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        integrate_frames(ctx, forest->raw_rgb.get(), forest->raw_depth.get(), count, width, height, forest->color.get(),
+                         forest->depth.get());
+        std::vector<FrameDesc>& frames = forest->h_frames;
+        frames.resize(count);
+        for (int i = 0; i < count; i++) {
+            FrameDesc& fr = frames[i];
+            fr.color = forest->color.get() + plane * 3 * i;
+            fr.depth = forest->depth.get() + plane * i;
+            fr.probs = probabilities ? forest->probs.get() + plane * forest->C * i : nullptr;
+            fr.labels = forest->labels.get() + plane * i;
+            fr.width = width;
+            fr.height = height;
+            fr.pad = 0;
+        }
+        predict_frames(forest, frames);
+        if (probabilities)
+            CF_CUDA_CHECK(cudaMemcpyAsync(probabilities, forest->probs.get(), sizeof(float) * plane * forest->C * count,
+                                          cudaMemcpyDeviceToHost, ctx->stream));
+        if (labels)
+            CF_CUDA_CHECK(cudaMemcpyAsync(labels, forest->labels.get(), plane * count, cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,640 @@
+// Split search for a tree level (kernels b, c, d).
+//
+// Level-batched form: every open node of the level is cut into work items (node, feature range)
+// and one persistent launch drains the item queue. A CTA evaluates its item tile by tile:
+//   1. stage the tile's feature parameters, sorted thresholds and threshold ranks in shared memory;
+//   2. for every (sample, feature) pair compute the double response exactly as the reference does,
+//      locate it among the feature's sorted thresholds (binary search on the response rounded up
+//      to float, which orders identically to the reference's double compare) and increment ONE
+//      shared-memory bin [feature][class][position], warp-aggregated with __match_any_sync;
+//   3. turn the bins into cumulative counts, so left(t) = bins up to rank(t), right = node - left;
+//   4. score every (feature, threshold) with the normalised information gain in double and keep
+//      the near-best candidates; a final per-node reduction applies the tie rule.
+// Counts never leave the SM; only the candidates of each item do.
+//
+// Per-node form: the reference's structure (random_tree_image_gpu.cu:1455-1720, 2137-2182):
+// responses [F][N] to global memory, one block per (threshold, feature) histogramming them,
+// a score kernel and a host argmax, launched node by node.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "split_eval.h"
+
+namespace cf {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int bin_of(double r, const float* sorted, int T) {
+    if (isnan(r)) return T;
+    const float ru = __double2float_ru(r);
+    int lo = 0, n = T;
+    while (n > 0) {
+        const int half = n >> 1;
+        if (sorted[lo + half] < ru) {
+            lo += half + 1;
+            n -= half + 1;
+        } else {
+            n = half;
+        }
+    }
+    return lo;
+}
+
+template <bool kAgg>
+__device__ __forceinline__ void bin_increment(uint32_t* bins, int key) {
+    if (kAgg) {
+        const unsigned peers = __match_any_sync(kFull, key);
+        const int leader = __ffs(peers) - 1;
+        if (key >= 0 && static_cast<int>(threadIdx.x & 31) == leader) atomicAdd(bins + key, __popc(peers));
+    } else {
+        if (key >= 0) atomicAdd(bins + key, 1u);
+    }
+}
+
+struct EvalArgs {
+    DsView ds;
+    const Sample* samples;
+    const NodeDesc* nodes;
+    const uint32_t* node_hist;
+    int C, F, T;
+    const FeatParams* packs;
+    const float* sorted_thr;
+    const uint16_t* ranks;
+    const EvalItem* items;
+    const int* order;
+    int n_items;
+    int* queue;
+    ItemCandidates* cands;
+    int ft_max;
+    int bins_budget;
+};
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+struct SmemLayout {
+    size_t counts, params, thr, rank, scores, bins, total;
+    __host__ __device__ SmemLayout(int C, int T, int ft_max, int budget) {
+        size_t o = 0;
+        counts = o;
+        o += align16(sizeof(uint32_t) * C);
+        params = o;
+        o += align16(sizeof(FeatParams) * ft_max);
+        thr = o;
+        o += align16(sizeof(float) * ft_max * T);
+        rank = o;
+        o += align16(sizeof(uint16_t) * ft_max * T);
+        scores = o;
+        o += align16(sizeof(double) * ft_max * T);
+        bins = o;
+        o += align16(sizeof(uint32_t) * budget);
+        total = o;
+    }
+};
+
+// Normalised information gain of one (feature, threshold) from cumulative bins.
+// cum points at bins[f][0][rank]; stride between classes is T + 1.
+__device__ inline double score_from_cum(const uint32_t* cum, int stride, const uint32_t* counts, int cp, double total,
+                                        double hc) {
+    uint32_t L = 0;
+    for (int i = 0; i < cp; i++) L += cum[i * stride];
+    const double Ld = static_cast<double>(L);
+    const double Rd = __dsub_rn(total, Ld);
+    if (L == 0 || Rd == 0.0) return 0.0;
+    const double leftProb = __ddiv_rn(Ld, total);
+    const double rightProb = __ddiv_rn(Rd, total);
+    double ig = 0;
+    for (int i = 0; i < cp; i++) {
+        const uint32_t h = counts[i];
+        const uint32_t l = cum[i * stride];
+        const uint32_t r = h - l;
+        const double classProb = __ddiv_rn(static_cast<double>(h), total);
+        if (l > 0) ig = __dadd_rn(ig, ig_term(static_cast<double>(l), total, leftProb, classProb));
+        if (r > 0) ig = __dadd_rn(ig, ig_term(static_cast<double>(r), total, rightProb, classProb));
+    }
+    ig = normalize_score(ig);
+    if (ig == 0) return 0.0;
+    const double hs = __ddiv_rn(__dsub_rn(__dadd_rn(entropy_of(Ld), entropy_of(Rd)), entropy_of(total)), total);
+    return normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, hc)));
+}
+
+template <bool kAgg>
+__global__ void __launch_bounds__(256)
+level_eval_kernel(EvalArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_item;
+    __shared__ uint8_t s_lid[256];
+    __shared__ int s_warp_cnt[8];
+    __shared__ int s_cp;
+    __shared__ double s_total, s_hc;
+    __shared__ double s_best;
+    __shared__ double s_cs[kMaxCand];
+    __shared__ int s_ct[kMaxCand], s_cf[kMaxCand];
+    __shared__ int s_cn, s_ovf;
+
+    const SmemLayout L(a.C, a.T, a.ft_max, a.bins_budget);
+    uint32_t* s_counts = reinterpret_cast<uint32_t*>(smem + L.counts);
+    FeatParams* s_params = reinterpret_cast<FeatParams*>(smem + L.params);
+    float* s_thr = reinterpret_cast<float*>(smem + L.thr);
+    uint16_t* s_rank = reinterpret_cast<uint16_t*>(smem + L.rank);
+    double* s_scores = reinterpret_cast<double*>(smem + L.scores);
+    uint32_t* s_bins = reinterpret_cast<uint32_t*>(smem + L.bins);
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int T = a.T;
+    const int T1 = T + 1;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int q = s_item;
+        if (q >= a.n_items) return;
+        const int item_id = a.order[q];
+        const EvalItem item = a.items[item_id];
+        const NodeDesc nd = a.nodes[item.node];
+        const uint32_t* hist = a.node_hist + static_cast<long long>(item.node) * a.C;
+
+        // ---- class compaction: present classes get dense ids in ascending label order
+        {
+            const uint32_t cnt = tid < a.C ? hist[tid] : 0u;
+            const bool present = cnt > 0;
+            const unsigned bal = __ballot_sync(kFull, present);
+            if (lane == 0) s_warp_cnt[warp] = __popc(bal);
+            __syncthreads();
+            int base = 0;
+            for (int w = 0; w < warp; w++) base += s_warp_cnt[w];
+            const int idx = base + __popc(bal & ((1u << lane) - 1u));
+            if (tid < 256) s_lid[tid] = present ? static_cast<uint8_t>(idx) : static_cast<uint8_t>(255);
+            if (present) s_counts[idx] = cnt;
+            if (tid == 0) {
+                int cp = 0;
+                for (int w = 0; w < 8; w++) cp += s_warp_cnt[w];
+                s_cp = cp;
+                s_best = -INFINITY;
+                s_cn = 0;
+                s_ovf = 0;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                // node total and classification entropy, classes in ascending label order (score.h:174-189)
+                double total = 0;
+                for (int i = 0; i < s_cp; i++) total += static_cast<double>(s_counts[i]);
+                s_total = total;
+                s_hc = classification_entropy(s_cp, s_counts, total);
+            }
+            __syncthreads();
+        }
+        const int cp = s_cp;
+        const double total = s_total;
+        const double hc = s_hc;
+        const int N = nd.count;
+        int ft = a.bins_budget / (cp * T1);
+        ft = max(1, min(ft, a.ft_max));
+
+        for (int f0 = item.f_begin; f0 < item.f_end; f0 += ft) {
+            const int nf = min(ft, item.f_end - f0);
+            // ---- stage the tile
+            for (int i = tid; i < nf; i += blockDim.x) s_params[i] = a.packs[f0 + i];
+            for (int i = tid; i < nf * T; i += blockDim.x) {
+                s_thr[i] = a.sorted_thr[static_cast<long long>(f0) * T + i];
+                s_rank[i] = a.ranks[static_cast<long long>(f0) * T + i];
+            }
+            const int nbins = nf * cp * T1;
+            for (int i = tid; i < nbins; i += blockDim.x) s_bins[i] = 0u;
+            __syncthreads();
+
+            // ---- histogram: pairs p = f * N + s, uniform trip count so warps stay converged
+            const long long pairs = static_cast<long long>(nf) * N;
+            const int iters = static_cast<int>((pairs + blockDim.x - 1) / blockDim.x);
+            const int stride = blockDim.x;
+            const int qstep = stride / N;
+            const int rstep = stride - qstep * N;
+            int f = tid / N;
+            int s = tid - f * N;
+            for (int it = 0; it < iters; it++) {
+                int key1 = -1, key2 = -1;
+                if (f < nf) {
+                    const Sample smp = a.samples[nd.start + s];
+                    const FeatParams fp = s_params[f];
+                    const float* sorted = s_thr + f * T;
+                    const int row = (f * cp + s_lid[smp.label]) * T1;
+                    if (smp.flip == 2) {
+                        key1 = row + bin_of(sample_response(a.ds, smp, fp, false), sorted, T);
+                        key2 = row + bin_of(sample_response(a.ds, smp, fp, true), sorted, T);
+                    } else {
+                        key1 = row + bin_of(sample_response(a.ds, smp, fp, smp.flip == 1), sorted, T);
+                    }
+                }
+                bin_increment<kAgg>(s_bins, key1);
+                if (__any_sync(kFull, key2 >= 0)) bin_increment<kAgg>(s_bins, key2);
+                s += rstep;
+                f += qstep;
+                if (s >= N) {
+                    s -= N;
+                    f++;
+                }
+            }
+            __syncthreads();
+
+            // ---- cumulative counts along the threshold positions
+            for (int row = tid; row < nf * cp; row += blockDim.x) {
+                uint32_t acc = 0;
+                uint32_t* b = s_bins + row * T1;
+                for (int k = 0; k < T1; k++) {
+                    acc += b[k];
+                    b[k] = acc;
+                }
+            }
+            __syncthreads();
+
+            // ---- scores of every (feature, threshold) of the tile
+            for (int i = tid; i < nf * T; i += blockDim.x) {
+                const int fl = i / T;
+                const int t = i - fl * T;
+                const int rank = s_rank[fl * T + t];
+                s_scores[i] = score_from_cum(s_bins + fl * cp * T1 + rank, T1, s_counts, cp, total, hc);
+            }
+            __syncthreads();
+
+            // ---- near-best candidates (warp 0): window rule best - s < 1e-13, lowest (t, f) first
+            if (warp == 0) {
+                const int n = nf * T;
+                double m = -INFINITY;
+                for (int i = lane; i < n; i += 32) m = fmax(m, s_scores[i]);
+                for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(kFull, m, off));
+                const double mnew = fmax(m, s_best);
+                if (lane == 0) {
+                    int k = 0;
+                    for (int j = 0; j < s_cn; j++) {
+                        if (__dsub_rn(mnew, s_cs[j]) < 1e-13) {
+                            s_cs[k] = s_cs[j];
+                            s_ct[k] = s_ct[j];
+                            s_cf[k] = s_cf[j];
+                            k++;
+                        }
+                    }
+                    s_cn = k;
+                    s_best = mnew;
+                }
+                __syncwarp();
+                for (int base = 0; base < n; base += 32) {
+                    const int i = base + lane;
+                    const bool e = i < n && __dsub_rn(mnew, s_scores[i]) < 1e-13;
+                    unsigned bal = __ballot_sync(kFull, e);
+                    if (lane == 0) {
+                        while (bal) {
+                            const int b = __ffs(bal) - 1;
+                            bal &= bal - 1;
+                            const int ii = base + b;
+                            const int fl = ii / T;
+                            const int t = ii - fl * T;
+                            const int fg = f0 + fl;
+                            const long long key = static_cast<long long>(t) * a.F + fg;
+                            int pos = s_cn;
+                            while (pos > 0 && static_cast<long long>(s_ct[pos - 1]) * a.F + s_cf[pos - 1] > key) pos--;
+                            if (pos >= kMaxCand) {
+                                s_ovf = 1;
+                                continue;
+                            }
+                            if (s_cn == kMaxCand) s_ovf = 1;
+                            const int last = min(s_cn, kMaxCand - 1);
+                            for (int j = last; j > pos; j--) {
+                                s_cs[j] = s_cs[j - 1];
+                                s_ct[j] = s_ct[j - 1];
+                                s_cf[j] = s_cf[j - 1];
+                            }
+                            s_cs[pos] = s_scores[ii];
+                            s_ct[pos] = t;
+                            s_cf[pos] = fg;
+                            s_cn = min(s_cn + 1, kMaxCand);
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+        }
+
+        if (tid == 0) {
+            ItemCandidates c;
+            c.best = s_best;
+            c.n = s_cn;
+            c.overflow = s_ovf;
+            for (int j = 0; j < kMaxCand; j++) {
+                c.s[j] = j < s_cn ? s_cs[j] : -INFINITY;
+                c.t[j] = j < s_cn ? s_ct[j] : 0;
+                c.f[j] = j < s_cn ? s_cf[j] : 0;
+            }
+            a.cands[item_id] = c;
+        }
+    }
+}
+
+// One thread per node: global tie rule over the candidates of the node's items.
+__global__ void reduce_candidates_kernel(int M, int F, const int* __restrict__ item_range,
+                                         const ItemCandidates* __restrict__ cands, const float* __restrict__ thr,
+                                         cf_split* __restrict__ out) {
+    const int node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= M) return;
+    const int b = item_range[node], e = item_range[node + 1];
+    double m = -INFINITY;
+    int ovf = 0;
+    for (int i = b; i < e; i++) {
+        m = fmax(m, cands[i].best);
+        ovf |= cands[i].overflow;
+    }
+    long long best_key = LLONG_MAX;
+    double best_s = m;
+    int bt = 0, bf = 0;
+    for (int i = b; i < e; i++) {
+        const ItemCandidates& c = cands[i];
+        for (int j = 0; j < c.n; j++) {
+            if (__dsub_rn(m, c.s[j]) < 1e-13) {
+                const long long key = static_cast<long long>(c.t[j]) * F + c.f[j];
+                if (key < best_key) {
+                    best_key = key;
+                    best_s = c.s[j];
+                    bt = c.t[j];
+                    bf = c.f[j];
+                }
+            }
+        }
+    }
+    cf_split r;
+    r.score = best_s;
+    r.feature = bf;
+    r.threshold_index = bt;
+    r.threshold = thr[static_cast<long long>(bt) * F + bf];
+    r.flags = ovf;
+    out[node] = r;
+}
+
+// ---- reference-structured kernels --------------------------------------------------------------
+
+// featureResponseKernel layout: block (4 samples, 32 features), responses [F][N]
+__global__ void plain_response_kernel(DsView ds, const Sample* __restrict__ samples, int N, const int8_t* __restrict__ table,
+                                      int F, double* __restrict__ resp1, double* __restrict__ resp2) {
+    const int feature = blockIdx.x * blockDim.y + threadIdx.y;
+    const int sample = blockIdx.y * blockDim.x + threadIdx.x;
+    if (feature >= F || sample >= N) return;
+    const FeatParams fp = load_feature(table, F, feature);
+    const Sample s = samples[sample];
+    const long long o = static_cast<long long>(feature) * N + sample;
+    resp1[o] = sample_response(ds, s, fp, s.flip == 1);
+    if (s.flip == 2 && resp2) resp2[o] = sample_response(ds, s, fp, true);
+}
+
+// aggregateHistogramsKernel structure: one block per (threshold, feature); per-label left/right
+// counters in shared memory (uint32, any number of classes), added into counters [F][T][C][2].
+__global__ void plain_histogram_kernel(const double* __restrict__ resp1, const double* __restrict__ resp2,
+                                       const Sample* __restrict__ samples, int N, const float* __restrict__ thr, int F,
+                                       int T, int C, uint32_t* __restrict__ counters) {
+    extern __shared__ uint32_t s_cnt[];
+    const int thresh = blockIdx.x;
+    const int feature = blockIdx.y;
+    const float threshold = thr[static_cast<long long>(thresh) * F + feature];
+    for (int i = threadIdx.x; i < 2 * C; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    const double* r1 = resp1 + static_cast<long long>(feature) * N;
+    const double* r2 = resp2 ? resp2 + static_cast<long long>(feature) * N : nullptr;
+    for (int s = threadIdx.x; s < N; s += blockDim.x) {
+        const Sample smp = samples[s];
+        const int v = !(r1[s] <= threshold);
+        atomicAdd(&s_cnt[2 * smp.label + v], 1u);
+        if (smp.flip == 2) {
+            const int v2 = !(r2[s] <= threshold);
+            atomicAdd(&s_cnt[2 * smp.label + v2], 1u);
+        }
+    }
+    __syncthreads();
+    uint32_t* out = counters + (static_cast<long long>(feature) * T + thresh) * C * 2;
+    for (int i = threadIdx.x; i < 2 * C; i += blockDim.x) out[i] += s_cnt[i];
+}
+
+// scoreKernel: one thread per (threshold, feature); scores [T][F]
+__global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const uint32_t* __restrict__ hist, int C, int F,
+                                   int T, double* __restrict__ scores) {
+    __shared__ double s_hc;
+    __shared__ double s_total;
+    if (threadIdx.x == 0) {
+        double total = 0, hc = 0;
+        for (int c = 0; c < C; c++) total += static_cast<double>(hist[c]);
+        for (int c = 0; c < C; c++)
+            if (hist[c] > 0) hc = __dadd_rn(hc, entropy_of(static_cast<double>(hist[c])));
+        hc = __dsub_rn(hc, entropy_of(total));
+        s_hc = __ddiv_rn(hc, total);
+        s_total = total;
+    }
+    __syncthreads();
+    const int feature = blockIdx.x * blockDim.x + threadIdx.x;
+    const int thresh = blockIdx.y;
+    if (feature >= F) return;
+    const uint32_t* lr = counters + (static_cast<long long>(feature) * T + thresh) * C * 2;
+    double Ld = 0, Rd = 0;
+    for (int c = 0; c < C; c++) {
+        Ld += static_cast<double>(lr[2 * c]);
+        Rd += static_cast<double>(lr[2 * c + 1]);
+    }
+    const double total = __dadd_rn(Ld, Rd);
+    double score = 0.0;
+    if (Ld != 0.0 && Rd != 0.0) {
+        const double leftProb = __ddiv_rn(Ld, total);
+        const double rightProb = __ddiv_rn(Rd, total);
+        double ig = 0;
+        for (int c = 0; c < C; c++) {
+            const uint32_t l = lr[2 * c], r = lr[2 * c + 1];
+            const double classProb = __ddiv_rn(static_cast<double>(hist[c]), total);
+            if (l > 0) ig = __dadd_rn(ig, ig_term(static_cast<double>(l), total, leftProb, classProb));
+            if (r > 0) ig = __dadd_rn(ig, ig_term(static_cast<double>(r), total, rightProb, classProb));
+        }
+        ig = normalize_score(ig);
+        if (ig != 0) {
+            const double hs =
+                __ddiv_rn(__dsub_rn(__dadd_rn(entropy_of(Ld), entropy_of(Rd)), entropy_of(total)), total);
+            score = normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, s_hc)));
+        }
+    }
+    scores[static_cast<long long>(thresh) * F + feature] = score;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
+                              const uint32_t* node_hist_dev, int M, const std::vector<int>& node_counts, int C,
+                              const LevelFeatures& lf, cf_split* splits_dev) {
+    const int F = lf.F, T = lf.T;
+    CF_REQUIRE(C >= 1 && C <= 256, "number of classes must be in [1, 256]");
+    CF_REQUIRE(T >= 1 && T <= 4096, "number of thresholds must be in [1, 4096]");
+    if (M == 0) return;
+    // work items: feature ranges sized so that the level yields ~items_per_slot items per resident CTA
+    long long total_work = 0;
+    for (int n : node_counts) total_work += static_cast<long long>(n) * F;
+    const int slots = ctx->num_sms * tuning.ctas_per_sm;
+    const double target_items = tuning.items_per_slot * slots;
+    const double work_per_item = std::max(1.0, static_cast<double>(total_work) / target_items);
+    h_items_.clear();
+    h_range_.assign(M + 1, 0);
+    std::vector<long long> item_work;
+    for (int n = 0; n < M; n++) {
+        h_range_[n] = static_cast<int>(h_items_.size());
+        const double w = static_cast<double>(node_counts[n]) * F;
+        int parts = static_cast<int>(std::ceil(w / work_per_item));
+        parts = std::max(1, std::min(parts, (F + 7) / 8));
+        int per = (F + parts - 1) / parts;
+        per = ((per + 7) / 8) * 8;
+        for (int f0 = 0; f0 < F; f0 += per) {
+            EvalItem it;
+            it.node = n;
+            it.f_begin = f0;
+            it.f_end = std::min(F, f0 + per);
+            it.pad = 0;
+            h_items_.push_back(it);
+            item_work.push_back(static_cast<long long>(node_counts[n]) * (it.f_end - it.f_begin));
+        }
+    }
+    h_range_[M] = static_cast<int>(h_items_.size());
+    const int n_items = static_cast<int>(h_items_.size());
+    h_order_.resize(n_items);
+    for (int i = 0; i < n_items; i++) h_order_[i] = i;
+    std::stable_sort(h_order_.begin(), h_order_.end(), [&](int x, int y) { return item_work[x] > item_work[y]; });
+    items_.reserve(n_items);
+    order_.reserve(n_items);
+    item_range_.reserve(M + 1);
+    cands_.reserve(n_items);
+    queue_.reserve(1);
+    CF_CUDA_CHECK(cudaMemcpyAsync(items_.get(), h_items_.data(), sizeof(EvalItem) * n_items, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CF_CUDA_CHECK(cudaMemcpyAsync(order_.get(), h_order_.data(), sizeof(int) * n_items, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CF_CUDA_CHECK(cudaMemcpyAsync(item_range_.get(), h_range_.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int), ctx->stream));
+    last_items = n_items;
+
+    int budget = tuning.bins_budget_words;
+    budget = std::max(budget, C * (T + 1));
+    const SmemLayout lay(C, T, tuning.ft_max, budget);
+    CF_REQUIRE(lay.total + 4096 <= ctx->smem_per_block_optin,
+               "split search: classes x thresholds too large for shared memory");
+    EvalArgs args;
+    args.ds = ds;
+    args.samples = samples;
+    args.nodes = nodes_dev;
+    args.node_hist = node_hist_dev;
+    args.C = C;
+    args.F = F;
+    args.T = T;
+    args.packs = lf.packs.get();
+    args.sorted_thr = lf.sorted_thr.get();
+    args.ranks = lf.ranks.get();
+    args.items = items_.get();
+    args.order = order_.get();
+    args.n_items = n_items;
+    args.queue = queue_.get();
+    args.cands = cands_.get();
+    args.ft_max = tuning.ft_max;
+    args.bins_budget = budget;
+    const int grid = std::min(n_items, slots);
+    if (tuning.warp_aggregate) {
+        CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(lay.total)));
+        launch(ctx, "level_eval", dim3(grid), dim3(256), lay.total, level_eval_kernel<true>, args);
+    } else {
+        CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(lay.total)));
+        launch(ctx, "level_eval", dim3(grid), dim3(256), lay.total, level_eval_kernel<false>, args);
+    }
+    launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F,
+           item_range_.get(), cands_.get(), lf.thr.get(), splits_dev);
+}
+
+void plain_responses(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start, int count,
+                     const int8_t* feat_table, int F, double* resp1, double* resp2) {
+    const unsigned fpb = std::min(F, 32);
+    const unsigned spb = std::min(count, 4);
+    dim3 grid((F + fpb - 1) / fpb, (count + spb - 1) / spb);
+    launch(ctx, "plain_response", grid, dim3(spb, fpb), 0, plain_response_kernel, ds, samples_dev + start, count,
+           feat_table, F, resp1, resp2);
+}
+
+void plain_scores(cf_context* ctx, int C, int F, int T, const uint32_t* counters, const uint32_t* node_hist,
+                  double* scores) {
+    const int tpb = std::min(F, 128);
+    launch(ctx, "plain_score", dim3((F + tpb - 1) / tpb, T), dim3(tpb), 0, plain_score_kernel, counters, node_hist, C,
+           F, T, scores);
+}
+
+void PlainNodeEvaluator::histograms(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start,
+                                    int count, int C, const int8_t* feat_table, const float* thr, int F, int T,
+                                    int max_batch) {
+    counters.reserve(static_cast<size_t>(F) * T * C * 2);
+    CF_CUDA_CHECK(cudaMemsetAsync(counters.get(), 0, sizeof(uint32_t) * F * T * C * 2, ctx->stream));
+    if (max_batch <= 0) max_batch = 50000;
+    const int batch = std::min(count, max_batch);
+    resp1.reserve(static_cast<size_t>(F) * batch);
+    resp2.reserve(static_cast<size_t>(F) * batch);
+    for (int b = 0; b < count; b += batch) {
+        const int n = std::min(batch, count - b);
+        plain_responses(ctx, ds, samples_dev, start + b, n, feat_table, F, resp1.get(), resp2.get());
+        const int tpb = n <= 3000 ? 64 : 128;
+        launch(ctx, "plain_histogram", dim3(T, F), dim3(tpb), sizeof(uint32_t) * 2 * C, plain_histogram_kernel,
+               resp1.get(), resp2.get(), samples_dev + start + b, n, thr, F, T, C, counters.get());
+    }
+}
+
+void host_window_argmax(const double* scores, int F, int T, int* best_f, int* best_t, double* best_s) {
+    double m = -std::numeric_limits<double>::infinity();
+    for (long long i = 0; i < static_cast<long long>(F) * T; i++) m = std::max(m, scores[i]);
+    *best_f = 0;
+    *best_t = 0;
+    *best_s = m;
+    for (int t = 0; t < T; t++)
+        for (int f = 0; f < F; f++) {
+            const double s = scores[static_cast<long long>(t) * F + f];
+            if (m - s < 1e-13) {
+                *best_f = f;
+                *best_t = t;
+                *best_s = s;
+                return;
+            }
+        }
+}
+
+void PlainNodeEvaluator::evaluate_node(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start,
+                                       int count, const uint32_t* node_hist_dev, int C, const LevelFeatures& lf,
+                                       int max_batch, cf_split* split_dev_out, cf_split* split_host_out) {
+    const int F = lf.F, T = lf.T;
+    histograms(ctx, ds, samples_dev, start, count, C, lf.feat.get(), lf.thr.get(), F, T, max_batch);
+    scores.reserve(static_cast<size_t>(F) * T);
+    plain_scores(ctx, C, F, T, counters.get(), node_hist_dev, scores.get());
+    h_scores.resize(static_cast<size_t>(F) * T);
+    CF_CUDA_CHECK(cudaMemcpyAsync(h_scores.data(), scores.get(), sizeof(double) * F * T, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    int bf, bt;
+    double bs;
+    host_window_argmax(h_scores.data(), F, T, &bf, &bt, &bs);
+    float thr;
+    CF_CUDA_CHECK(cudaMemcpy(&thr, lf.thr.get() + static_cast<long long>(bt) * F + bf, sizeof(float),
+                             cudaMemcpyDeviceToHost));
+    cf_split r;
+    r.score = bs;
+    r.feature = bf;
+    r.threshold_index = bt;
+    r.threshold = thr;
+    r.flags = 0;
+    if (split_host_out) *split_host_out = r;
+    if (split_dev_out)
+        CF_CUDA_CHECK(cudaMemcpyAsync(split_dev_out, &r, sizeof(cf_split), cudaMemcpyHostToDevice, ctx->stream));
+    CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace cf

@@ -1,0 +1,90 @@
+// Split search of one tree level: the level-batched persistent kernel and the reference-structured
+// per-node kernels.
+#pragma once
+
+#include "features.h"
+
+namespace cf {
+
+// One open node of a level: its samples are [start, start + count) of the level's sample array.
+struct NodeDesc {
+    long long start;
+    int count;
+    int tree_index;
+};
+
+struct EvalItem {
+    int node;
+    int f_begin;
+    int f_end;
+    int pad;
+};
+
+constexpr int kMaxCand = 4;
+
+// Near-best candidates of one work item: every entry has best - score < 1e-13, sorted by
+// (threshold, feature), at most kMaxCand lowest indices (overflow set when more existed).
+struct ItemCandidates {
+    double best;
+    double s[kMaxCand];
+    int t[kMaxCand];
+    int f[kMaxCand];
+    int n;
+    int overflow;
+};
+
+struct EvalTuning {
+    int threads = 256;
+    int ft_max = 32;              // features per tile upper bound
+    int bins_budget_words = 12288;  // shared-memory histogram budget per CTA (u32 words)
+    int warp_aggregate = 1;       // __match_any_sync aggregation of the shared-memory increments
+    int ctas_per_sm = 3;
+    double items_per_slot = 4.0;  // work items per resident CTA for load balance
+};
+
+class LevelEvaluator {
+public:
+    // nodes_dev / node_hist_dev: M node descriptors and [M][C] histograms on the device;
+    // node_counts: the M sample counts on the host (for work-item sizing).
+    void evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
+                  const uint32_t* node_hist_dev, int M, const std::vector<int>& node_counts, int C,
+                  const LevelFeatures& lf, cf_split* splits_dev);
+    EvalTuning tuning;
+    int64_t last_items = 0;
+
+private:
+    DevArray<EvalItem> items_;
+    DevArray<int> order_;
+    DevArray<int> item_range_;   // [M + 1] first item of each node
+    DevArray<ItemCandidates> cands_;
+    DevArray<int> queue_;
+    std::vector<EvalItem> h_items_;
+    std::vector<int> h_order_;
+    std::vector<int> h_range_;
+};
+
+// Reference-structured evaluation of one node (featureResponseKernel -> aggregateHistogramsKernel
+// -> scoreKernel -> host argmax), the "plain per-node" form.
+class PlainNodeEvaluator {
+public:
+    void evaluate_node(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start, int count,
+                       const uint32_t* node_hist_dev, int C, const LevelFeatures& lf, int max_batch,
+                       cf_split* split_dev_out, cf_split* split_host_out);
+    // counters [F][T][C][2] for samples on the device (accumulated over batches)
+    void histograms(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start, int count, int C,
+                    const int8_t* feat_table, const float* thr, int F, int T, int max_batch);
+    DevArray<uint32_t> counters;
+    DevArray<double> scores;
+    DevArray<double> resp1, resp2;
+    std::vector<double> h_scores;
+};
+
+void plain_responses(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start, int count,
+                     const int8_t* feat_table, int F, double* resp1, double* resp2);
+void plain_scores(cf_context* ctx, int C, int F, int T, const uint32_t* counters, const uint32_t* node_hist,
+                  double* scores);
+
+// Host window argmax: highest score, ties (best - s < 1e-13) to the lowest (threshold, feature).
+void host_window_argmax(const double* scores, int F, int T, int* best_f, int* best_t, double* best_s);
+
+}  // namespace cf

@@ -1,0 +1,472 @@
+// Breadth-first tree training on the GPU (RandomTreeTrain::train, random_tree.h:1249-1415, with
+// ImageFeatureEvaluation::evaluateBestSplits, random_tree_image.cpp:239-502) and the
+// ImageFeatureEvaluation entry points of the C-ABI.
+//
+// Per level, all on the device: candidate generation from the level's samples, the split search
+// (level-batched persistent launch, or node by node in the reference's structure), and routing
+// into the next level's node-contiguous sample array. The host only draws the level seed, sizes
+// the work items from the node counts and checks the empty-child flag.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "host_rng.h"
+#include "route.h"
+#include "tree.h"
+
+namespace cf {
+
+namespace {
+
+void validate_config(const cf_train_config* cfg) {
+    CF_REQUIRE(cfg != nullptr, "training configuration is NULL");
+    CF_REQUIRE(cfg->feature_count >= 1, "featureCount must be >= 1");
+    CF_REQUIRE(cfg->thresholds >= 1, "thresholds must be >= 1");
+    CF_REQUIRE(cfg->max_depth >= 1, "maxDepth must be >= 1");
+    CF_REQUIRE(cfg->box_radius > 0, "boxRadius must be > 0");
+    CF_REQUIRE(cfg->region_size > 0, "regionSize must be > 0");
+    CF_REQUIRE(cfg->max_images <= 0 || cfg->max_images >= cfg->image_cache_size,
+               "illegal configuration: maxImages must not be lower than imageCacheSize");
+}
+
+void validate_samples(const cf_dataset* ds, const cf_sample* s, long long n, int C) {
+    for (long long i = 0; i < n; i++) {
+        CF_REQUIRE(s[i].image < static_cast<uint32_t>(ds->n), "sample " + std::to_string(i) + ": image index out of range");
+        CF_REQUIRE(s[i].x < ds->width && s[i].y < ds->height, "sample " + std::to_string(i) + ": pixel outside the image");
+        CF_REQUIRE(s[i].label < C, "sample " + std::to_string(i) + ": label >= number of classes");
+        CF_REQUIRE(s[i].flip <= 2, "sample " + std::to_string(i) + ": unknown flip setting");
+    }
+}
+
+void validate_thresholds(const float* thr, long long n) {
+    for (long long i = 0; i < n; i++) CF_REQUIRE(!std::isnan(thr[i]), "thresholds must not be NaN");
+}
+
+}  // namespace
+
+class TreeTrainer {
+public:
+    TreeTrainer(cf_dataset* ds, int C, const cf_train_config& cfg, int mode) : ds_(ds), C_(C), cfg_(cfg), mode_(mode) {}
+
+    cf_tree* train(const cf_sample* host_samples, int N, int tree_id, int32_t* seed_counter) {
+        cf_context* ctx = ds_->ctx;
+        make_current(ctx);
+        CF_REQUIRE(N > 0, "training needs at least one sample");
+        CF_REQUIRE(C_ >= 1 && C_ <= 256, "number of classes must be in [1, 256]");
+        validate_samples(ds_, host_samples, N, C_);
+        const int F = static_cast<int>(cfg_.feature_count), T = cfg_.thresholds;
+        bool any_both = false;
+        std::vector<uint32_t> root_hist(C_, 0);
+        for (int i = 0; i < N; i++) {
+            root_hist[host_samples[i].label] += host_samples[i].flip == 2 ? 2 : 1;
+            any_both |= host_samples[i].flip == 2;
+        }
+        const long long cap = static_cast<long long>(N) * (any_both ? 2 : 1);
+        CF_REQUIRE(2 * cap + 1 < (1LL << 31), "too many samples for one tree");
+        samples_[0].reserve(cap);
+        samples_[1].reserve(cap);
+        snode_[0].reserve(cap);
+        snode_[1].reserve(cap);
+        nodes_[0].reserve(cap);
+        nodes_[1].reserve(cap);
+        hist_[0].reserve(static_cast<size_t>(cap) * C_);
+        hist_[1].reserve(static_cast<size_t>(cap) * C_);
+        splits_.reserve(cap);
+        tree_.reserve(static_cast<int>(2 * cap + 1), C_);
+        lf_.reserve(F, T);
+
+        cudaStream_t st = ctx->stream;
+        CF_CUDA_CHECK(cudaMemcpyAsync(samples_[0].get(), host_samples, sizeof(cf_sample) * N, cudaMemcpyHostToDevice, st));
+        CF_CUDA_CHECK(cudaMemsetAsync(snode_[0].get(), 0, sizeof(int) * N, st));
+        NodeDesc root{0, N, 0};
+        CF_CUDA_CHECK(cudaMemcpyAsync(nodes_[0].get(), &root, sizeof(NodeDesc), cudaMemcpyHostToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(hist_[0].get(), root_hist.data(), sizeof(uint32_t) * C_, cudaMemcpyHostToDevice, st));
+        // root record
+        {
+            const int32_t lvl = 1, lft = -1, fid = -1;
+            const float nanf = std::nanf("");
+            const double nand = std::nan("");
+            const uint32_t ns = N;
+            int8_t zeros[11] = {0};
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.level.get(), &lvl, 4, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.left.get(), &lft, 4, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.feature_id.get(), &fid, 4, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.threshold.get(), &nanf, 4, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.score.get(), &nand, 8, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.nsamp.get(), &ns, 4, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.feature.get(), zeros, 11, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(tree_.hist.get(), root_hist.data(), sizeof(uint32_t) * C_, cudaMemcpyHostToDevice, st));
+        }
+        cudaEvent_t ev0, ev1;
+        CF_CUDA_CHECK(cudaEventCreate(&ev0));
+        CF_CUDA_CHECK(cudaEventCreate(&ev1));
+        CF_CUDA_CHECK(cudaEventRecord(ev0, st));
+
+        const DsView ds = view_of(ds_);
+        RandomSource rs(seed_counter);
+        int cur = 0;
+        int M = 1;
+        long long n = N;
+        int level = 1;
+        int tree_next = 1;
+        int64_t evals = 0;
+        int levels = 0;
+        std::vector<NodeDesc> h_nodes;
+        std::vector<int> counts;
+        while (M > 0 && level < cfg_.max_depth) {
+            // evaluateBestSplits: one seed per level from the tree's random source
+            const uint32_t seed = static_cast<uint32_t>(rs.uniform(0xFFFFFF).next());
+            generate_level_features(ctx, ds, samples_[cur].get(), static_cast<uint32_t>(n), seed, cfg_.box_radius,
+                                    cfg_.region_size, cfg_.use_depth_images, lf_);
+            h_nodes.resize(M);
+            CF_CUDA_CHECK(cudaMemcpyAsync(h_nodes.data(), nodes_[cur].get(), sizeof(NodeDesc) * M,
+                                          cudaMemcpyDeviceToHost, st));
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            counts.resize(M);
+            for (int i = 0; i < M; i++) counts[i] = h_nodes[i].count;
+            if (mode_ == CF_TRAIN_PER_NODE) {
+                for (int i = 0; i < M; i++)
+                    plain_.evaluate_node(ctx, ds, samples_[cur].get(), h_nodes[i].start, h_nodes[i].count,
+                                         hist_[cur].get() + static_cast<size_t>(i) * C_, C_, lf_,
+                                         static_cast<int>(cfg_.max_samples_per_batch), splits_.get() + i, nullptr);
+            } else {
+                eval_.evaluate(ctx, ds, samples_[cur].get(), nodes_[cur].get(), hist_[cur].get(), M, counts, C_, lf_,
+                               splits_.get());
+            }
+            evals += n * F;
+            levels++;
+            const bool scatter = level + 1 < cfg_.max_depth;
+            const int nxt = 1 - cur;
+            RouteResult rr = route_level(ctx, ds, samples_[cur].get(), snode_[cur].get(), n, nodes_[cur].get(), M,
+                                         splits_.get(), lf_, C_, level, static_cast<int>(cfg_.min_sample_count),
+                                         tree_next, scatter, tree_, rb_, scan_, samples_[nxt].get(), snode_[nxt].get(),
+                                         nodes_[nxt].get(), hist_[nxt].get());
+            if (rr.empty_child) {
+                cudaEventDestroy(ev0);
+                cudaEventDestroy(ev1);
+                fail(CF_ERR_EMPTY_CHILD, "no samples in left or right node (tree " + std::to_string(tree_id) +
+                                             ", level " + std::to_string(level) + ")");
+            }
+            tree_next += 2 * M;
+            if (!scatter) break;
+            cur = nxt;
+            M = rr.next_nodes;
+            n = rr.next_samples;
+            level++;
+        }
+        CF_CUDA_CHECK(cudaEventRecord(ev1, st));
+        CF_CUDA_CHECK(cudaEventSynchronize(ev1));
+        float ms = 0;
+        CF_CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+
+        auto* t = new cf_tree();
+        t->tree_id = tree_id;
+        t->C = C_;
+        t->resize(tree_next);
+        const int nn = tree_next;
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->level.data(), tree_.level.get(), 4 * nn, cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->left.data(), tree_.left.get(), 4 * nn, cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->feature_id.data(), tree_.feature_id.get(), 4 * nn, cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->feature.data(), tree_.feature.get(), 11 * static_cast<size_t>(nn),
+                                      cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->threshold.data(), tree_.threshold.get(), 4 * nn, cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->score.data(), tree_.score.get(), 8 * nn, cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->hist.data(), tree_.hist.get(), sizeof(uint32_t) * C_ * static_cast<size_t>(nn),
+                                      cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(t->nsamp.data(), tree_.nsamp.get(), 4 * nn, cudaMemcpyDeviceToHost, st));
+        CF_CUDA_CHECK(cudaStreamSynchronize(st));
+        t->feature_evals = evals;
+        t->device_ms = ms;
+        t->levels = levels;
+        return t;
+    }
+
+    LevelEvaluator eval_;
+
+private:
+    cf_dataset* ds_;
+    int C_;
+    cf_train_config cfg_;
+    int mode_;
+    DevArray<cf_sample> samples_raw_;
+    DevArray<Sample> samples_[2];
+    DevArray<int> snode_[2];
+    DevArray<NodeDesc> nodes_[2];
+    DevArray<uint32_t> hist_[2];
+    DevArray<cf_split> splits_;
+    DevTree tree_;
+    LevelFeatures lf_;
+    RouteBuffers rb_;
+    Scanner scan_;
+    PlainNodeEvaluator plain_;
+};
+
+cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
+                    int32_t* seed_counter, int mode) {
+    TreeTrainer trainer(ds, C, cfg, mode);
+    return trainer.train(samples, N, tree_id, seed_counter);
+}
+
+}  // namespace cf
+
+// ================================================================================================
+// C-ABI
+// ================================================================================================
+using namespace cf;
+
+namespace {
+
+struct Uploaded {
+    DevArray<Sample> samples;
+    DevArray<int8_t> feat;
+    DevArray<float> thr;
+};
+
+void upload_samples(cf_context* ctx, DevArray<Sample>& dst, const cf_sample* src, long long n) {
+    dst.reserve(std::max<long long>(n, 1));
+    if (n > 0)
+        CF_CUDA_CHECK(cudaMemcpyAsync(dst.get(), src, sizeof(cf_sample) * n, cudaMemcpyHostToDevice, ctx->stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+cf_status cf_feature_responses(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_features,
+                               const int8_t* features, double* responses) {
+    return guard([&] {
+        CF_REQUIRE(ds && samples && features && responses, "cf_feature_responses: NULL argument");
+        CF_REQUIRE(num_samples > 0 && num_features > 0, "cf_feature_responses: empty input");
+        cf_context* ctx = ds->ctx;
+        make_current(ctx);
+        validate_samples(ds, samples, num_samples, 256);
+        Uploaded u;
+        upload_samples(ctx, u.samples, samples, num_samples);
+        u.feat.reserve(static_cast<size_t>(11) * num_features);
+        CF_CUDA_CHECK(cudaMemcpyAsync(u.feat.get(), features, 11 * static_cast<size_t>(num_features),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        DevArray<double> r1, r2;
+        r1.reserve(static_cast<size_t>(num_features) * num_samples);
+        r2.reserve(static_cast<size_t>(num_features) * num_samples);
+        plain_responses(ctx, view_of(ds), u.samples.get(), 0, num_samples, u.feat.get(), num_features, r1.get(), r2.get());
+        CF_CUDA_CHECK(cudaMemcpyAsync(responses, r1.get(), sizeof(double) * num_features * num_samples,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_histograms(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_features, int num_thresholds,
+                        const int8_t* features, const float* thresholds, int num_classes, uint32_t* counters) {
+    return guard([&] {
+        CF_REQUIRE(ds && samples && features && thresholds && counters, "cf_histograms: NULL argument");
+        CF_REQUIRE(num_samples > 0 && num_features > 0 && num_thresholds > 0, "cf_histograms: empty input");
+        CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_histograms: classes must be in [1, 256]");
+        cf_context* ctx = ds->ctx;
+        make_current(ctx);
+        validate_samples(ds, samples, num_samples, num_classes);
+        validate_thresholds(thresholds, static_cast<long long>(num_features) * num_thresholds);
+        Uploaded u;
+        upload_samples(ctx, u.samples, samples, num_samples);
+        u.feat.reserve(static_cast<size_t>(11) * num_features);
+        u.thr.reserve(static_cast<size_t>(num_thresholds) * num_features);
+        CF_CUDA_CHECK(cudaMemcpyAsync(u.feat.get(), features, 11 * static_cast<size_t>(num_features),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(u.thr.get(), thresholds, sizeof(float) * num_features * num_thresholds,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        PlainNodeEvaluator pe;
+        pe.histograms(ctx, view_of(ds), u.samples.get(), 0, num_samples, num_classes, u.feat.get(), u.thr.get(),
+                      num_features, num_thresholds, 50000);
+        CF_CUDA_CHECK(cudaMemcpyAsync(counters, pe.counters.get(),
+                                      sizeof(uint32_t) * num_features * num_thresholds * num_classes * 2,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_scores(cf_context* ctx, int num_classes, int num_features, int num_thresholds, const uint32_t* counters,
+                    const uint32_t* node_histogram, double* scores) {
+    return guard([&] {
+        CF_REQUIRE(ctx && counters && node_histogram && scores, "cf_scores: NULL argument");
+        CF_REQUIRE(num_classes >= 1 && num_features > 0 && num_thresholds > 0, "cf_scores: empty input");
+        make_current(ctx);
+        const size_t nc = static_cast<size_t>(num_features) * num_thresholds * num_classes * 2;
+        DevArray<uint32_t> c, h;
+        DevArray<double> s;
+        c.reserve(nc);
+        h.reserve(num_classes);
+        s.reserve(static_cast<size_t>(num_features) * num_thresholds);
+        CF_CUDA_CHECK(cudaMemcpyAsync(c.get(), counters, sizeof(uint32_t) * nc, cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(h.get(), node_histogram, sizeof(uint32_t) * num_classes, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        plain_scores(ctx, num_classes, num_features, num_thresholds, c.get(), h.get(), s.get());
+        CF_CUDA_CHECK(cudaMemcpyAsync(scores, s.get(), sizeof(double) * num_features * num_thresholds,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample* samples, uint32_t seed,
+                               int num_features, int num_thresholds, int box_radius, int region_size,
+                               int use_depth_images, int8_t* features, float* thresholds) {
+    return guard([&] {
+        CF_REQUIRE(ds && samples && features && thresholds, "cf_generate_features: NULL argument");
+        CF_REQUIRE(num_samples > 0 && num_features > 0 && num_thresholds > 0, "cf_generate_features: empty input");
+        cf_context* ctx = ds->ctx;
+        make_current(ctx);
+        validate_samples(ds, samples, num_samples, 256);
+        Uploaded u;
+        upload_samples(ctx, u.samples, samples, num_samples);
+        LevelFeatures lf;
+        lf.reserve(num_features, num_thresholds);
+        generate_level_features(ctx, view_of(ds), u.samples.get(), static_cast<uint32_t>(num_samples), seed, box_radius,
+                                region_size, use_depth_images, lf);
+        CF_CUDA_CHECK(cudaMemcpyAsync(features, lf.feat.get(), 11 * static_cast<size_t>(num_features),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(thresholds, lf.thr.get(), sizeof(float) * num_features * num_thresholds,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* node_offsets, const cf_sample* samples,
+                                  int num_classes, int num_features, int num_thresholds, const int8_t* features,
+                                  const float* thresholds, cf_split* best) {
+    return guard([&] {
+        CF_REQUIRE(ds && node_offsets && samples && features && thresholds && best, "cf_evaluate_best_splits: NULL argument");
+        CF_REQUIRE(num_nodes > 0 && num_features > 0 && num_thresholds > 0, "cf_evaluate_best_splits: empty input");
+        CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_evaluate_best_splits: classes must be in [1, 256]");
+        cf_context* ctx = ds->ctx;
+        make_current(ctx);
+        const long long n = node_offsets[num_nodes];
+        CF_REQUIRE(node_offsets[0] == 0 && n > 0, "cf_evaluate_best_splits: node offsets must start at 0");
+        validate_samples(ds, samples, n, num_classes);
+        validate_thresholds(thresholds, static_cast<long long>(num_features) * num_thresholds);
+        std::vector<NodeDesc> nodes(num_nodes);
+        std::vector<int> counts(num_nodes);
+        std::vector<uint32_t> hist(static_cast<size_t>(num_nodes) * num_classes, 0);
+        for (int i = 0; i < num_nodes; i++) {
+            CF_REQUIRE(node_offsets[i + 1] > node_offsets[i], "cf_evaluate_best_splits: every node needs samples");
+            nodes[i] = NodeDesc{node_offsets[i], static_cast<int>(node_offsets[i + 1] - node_offsets[i]), i};
+            counts[i] = nodes[i].count;
+            for (long long s = node_offsets[i]; s < node_offsets[i + 1]; s++)
+                hist[static_cast<size_t>(i) * num_classes + samples[s].label] += samples[s].flip == 2 ? 2 : 1;
+        }
+        Uploaded u;
+        upload_samples(ctx, u.samples, samples, n);
+        DevArray<NodeDesc> d_nodes;
+        DevArray<uint32_t> d_hist;
+        DevArray<cf_split> d_best;
+        d_nodes.reserve(num_nodes);
+        d_hist.reserve(hist.size());
+        d_best.reserve(num_nodes);
+        CF_CUDA_CHECK(cudaMemcpyAsync(d_nodes.get(), nodes.data(), sizeof(NodeDesc) * num_nodes, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(d_hist.get(), hist.data(), sizeof(uint32_t) * hist.size(), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        LevelFeatures lf;
+        lf.reserve(num_features, num_thresholds);
+        CF_CUDA_CHECK(cudaMemcpyAsync(lf.feat.get(), features, 11 * static_cast<size_t>(num_features),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(lf.thr.get(), thresholds, sizeof(float) * num_features * num_thresholds,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        prepare_eval_features(ctx, lf);
+        LevelEvaluator ev;
+        ev.evaluate(ctx, view_of(ds), u.samples.get(), d_nodes.get(), d_hist.get(), num_nodes, counts, num_classes, lf,
+                    d_best.get());
+        CF_CUDA_CHECK(cudaMemcpyAsync(best, d_best.get(), sizeof(cf_split) * num_nodes, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_train_tree(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                        const cf_train_config* config, int tree_id, int32_t* seed_counter, int mode, cf_tree** out) {
+    return guard([&] {
+        CF_REQUIRE(ds && samples && seed_counter && out, "cf_train_tree: NULL argument");
+        validate_config(config);
+        CF_REQUIRE(mode == CF_TRAIN_LEVEL_BATCHED || mode == CF_TRAIN_PER_NODE, "cf_train_tree: unknown mode");
+        *out = train_tree(ds, samples, num_samples, num_classes, *config, tree_id, seed_counter, mode);
+    });
+}
+
+cf_status cf_tree_info(cf_tree* tree, int* num_nodes, int* num_classes, int* depth, int* tree_id) {
+    return guard([&] {
+        CF_REQUIRE(tree, "cf_tree_info: tree is NULL");
+        if (num_nodes) *num_nodes = tree->num_nodes;
+        if (num_classes) *num_classes = tree->C;
+        if (depth) *depth = tree->depth();
+        if (tree_id) *tree_id = tree->tree_id;
+    });
+}
+
+cf_status cf_tree_export(cf_tree* tree, int32_t* level, int32_t* left, int8_t* feature, float* threshold, double* score,
+                         int32_t* feature_id, uint32_t* histogram, uint32_t* num_samples) {
+    return guard([&] {
+        CF_REQUIRE(tree, "cf_tree_export: tree is NULL");
+        const size_t n = tree->num_nodes;
+        if (level) std::memcpy(level, tree->level.data(), 4 * n);
+        if (left) std::memcpy(left, tree->left.data(), 4 * n);
+        if (feature) std::memcpy(feature, tree->feature.data(), 11 * n);
+        if (threshold) std::memcpy(threshold, tree->threshold.data(), 4 * n);
+        if (score) std::memcpy(score, tree->score.data(), 8 * n);
+        if (feature_id) std::memcpy(feature_id, tree->feature_id.data(), 4 * n);
+        if (histogram) std::memcpy(histogram, tree->hist.data(), 4 * n * tree->C);
+        if (num_samples) std::memcpy(num_samples, tree->nsamp.data(), 4 * n);
+    });
+}
+
+cf_status cf_tree_import(int tree_id, int num_nodes, int num_classes, const int32_t* level, const int32_t* left,
+                         const int8_t* feature, const float* threshold, const double* score, const int32_t* feature_id,
+                         const uint32_t* histogram, cf_tree** out) {
+    return guard([&] {
+        CF_REQUIRE(out && left && feature && threshold && histogram, "cf_tree_import: NULL argument");
+        CF_REQUIRE(num_nodes >= 1 && num_classes >= 1 && num_classes <= 256, "cf_tree_import: bad sizes");
+        for (int i = 0; i < num_nodes; i++)
+            CF_REQUIRE(left[i] == -1 || (left[i] > i && left[i] + 1 < num_nodes),
+                       "cf_tree_import: child index out of range at node " + std::to_string(i));
+        auto* t = new cf_tree();
+        t->tree_id = tree_id;
+        t->C = num_classes;
+        t->resize(num_nodes);
+        const size_t n = num_nodes;
+        std::memcpy(t->left.data(), left, 4 * n);
+        std::memcpy(t->feature.data(), feature, 11 * n);
+        std::memcpy(t->threshold.data(), threshold, 4 * n);
+        std::memcpy(t->hist.data(), histogram, 4 * n * num_classes);
+        if (level) std::memcpy(t->level.data(), level, 4 * n);
+        if (score) std::memcpy(t->score.data(), score, 8 * n);
+        else std::fill(t->score.begin(), t->score.end(), std::nan(""));
+        if (feature_id) std::memcpy(t->feature_id.data(), feature_id, 4 * n);
+        else std::fill(t->feature_id.begin(), t->feature_id.end(), -1);
+        for (size_t i = 0; i < n; i++) {
+            uint32_t s = 0;
+            for (int c = 0; c < num_classes; c++) s += histogram[i * num_classes + c];
+            t->nsamp[i] = s;
+        }
+        if (!level) {
+            std::fill(t->level.begin(), t->level.end(), 0);
+            t->level[0] = 1;
+            for (size_t i = 0; i < n; i++)
+                if (t->left[i] >= 0) t->level[t->left[i]] = t->level[t->left[i] + 1] = t->level[i] + 1;
+        }
+        *out = t;
+    });
+}
+
+cf_status cf_tree_destroy(cf_tree* tree) {
+    return guard([&] { delete tree; });
+}
+
+cf_status cf_tree_train_stats(cf_tree* tree, int64_t* feature_evals, double* device_ms, int* levels) {
+    return guard([&] {
+        CF_REQUIRE(tree, "cf_tree_train_stats: tree is NULL");
+        if (feature_evals) *feature_evals = tree->feature_evals;
+        if (device_ms) *device_ms = tree->device_ms;
+        if (levels) *levels = tree->levels;
+    });
+}
+
+}  // extern "C"

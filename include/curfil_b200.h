@@ -1,0 +1,268 @@
+/*
+ * curfil_b200 C-ABI: the drop-in boundary for CURFIL's random-forest training split search and
+ * dense per-pixel prediction, implemented with hand-written sm_100a CUDA kernels.
+ *
+ * Plain pointers and sizes only; every entry point returns a cf_status and records a message
+ * retrievable with cf_last_error(). Host buffers are owned by the caller. Device memory is owned
+ * by the objects (context, dataset, forest, server) that allocate it, except where a function
+ * says it takes device pointers. Each declaration names the reference interface it replaces
+ * (paths relative to the deeplearningais/curfil project root).
+ */
+#ifndef CURFIL_B200_H
+#define CURFIL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t cf_status;
+#define CF_OK 0
+#define CF_ERR_INVALID 1       /* bad argument or configuration (reference: std::runtime_error) */
+#define CF_ERR_CUDA 2          /* CUDA runtime error (reference: cudaSafeCall, utils.h:48) */
+#define CF_ERR_OOM 3           /* device allocation failed */
+#define CF_ERR_EMPTY_CHILD 4   /* "no samples in left/right node" (random_tree.h:1388-1393) */
+#define CF_ERR_CAPACITY 5      /* a fixed capacity was exceeded */
+#define CF_ERR_TIMEOUT 6       /* a bounded wait ran out */
+#define CF_ERR_REJECTED 7      /* serving admission refused the request */
+#define CF_ERR_IO 8            /* file read/write or format error */
+#define CF_ERR_STATE 9         /* object used in the wrong state */
+
+typedef struct cf_context cf_context;
+typedef struct cf_dataset cf_dataset;
+typedef struct cf_tree cf_tree;
+typedef struct cf_forest cf_forest;
+typedef struct cf_server cf_server;
+
+/* One pixel sample: PixelInstance (src/curfil/random_tree_image.h:140-181) with the image
+ * pointer replaced by an index into a dataset. 16 bytes. */
+typedef struct cf_sample {
+    uint16_t x, y;
+    uint32_t image;
+    float depth;      /* metres, Depth::getFloatValue() (image.h:146-149); <= 0 means invalid */
+    uint8_t label;
+    uint8_t flip;     /* HorizontalFlipSetting: 0 NoFlip, 1 Flip, 2 Both (random_tree.h:58-60) */
+    uint16_t reserved;
+} cf_sample;
+
+/* SplitFunction result of evaluateBestSplits (random_tree_image.cpp:445-471). */
+typedef struct cf_split {
+    double score;
+    int32_t feature;          /* index into the level's sorted candidate table */
+    int32_t threshold_index;
+    float threshold;
+    int32_t flags;            /* bit 0: more near-ties than the candidate lists hold (argmax exact only
+                                 up to the lowest four indices per work item) */
+} cf_split;
+
+/* TrainingConfiguration (random_tree.h:187-493), the fields the hot path reads. */
+typedef struct cf_train_config {
+    int32_t random_seed;
+    uint32_t samples_per_image;
+    uint32_t feature_count;
+    uint32_t min_sample_count;
+    int32_t max_depth;
+    uint16_t box_radius;        /* offset range ("boxRadius") */
+    uint16_t region_size;       /* box half-size range ("regionSize") */
+    uint16_t thresholds;
+    uint16_t reserved0;
+    int32_t num_threads;
+    int32_t max_images;
+    int32_t image_cache_size;
+    uint32_t max_samples_per_batch;
+    int32_t acceleration_mode;  /* 0 CPU_ONLY, 1 GPU_ONLY, 2 GPU_AND_CPU_COMPARE (random_tree.h:79-83) */
+    int32_t use_cie_lab;
+    int32_t use_depth_filling;
+    int32_t use_depth_images;
+    int32_t horizontal_flipping;
+    int32_t subsampling_type;   /* 0 classUniform, 1 pixelUniform */
+} cf_train_config;
+
+/* ---------------------------------------------------------------------------------------------
+ * Context and errors
+ * ------------------------------------------------------------------------------------------- */
+const char* cf_version(void);
+/* Message of the last failed call on this thread; returns its full length. */
+size_t cf_last_error(char* buffer, size_t length);
+/* Replaces selectDevice/initDevice and the global streams (random_tree_image_gpu.cu:55-56,1722-1770). */
+cf_status cf_context_create(int device, cf_context** out);
+cf_status cf_context_destroy(cf_context* ctx);
+/* Launch all work of this context on `stream` (a cudaStream_t); NULL restores the own stream. */
+cf_status cf_context_set_stream(cf_context* ctx, void* stream);
+cf_status cf_context_synchronize(cf_context* ctx);
+/* Per-kernel CUDA-event timing (replaces utils::Profile, utils.h:159-203). */
+cf_status cf_context_set_timing(cf_context* ctx, int enable);
+cf_status cf_context_kernel_time(cf_context* ctx, const char* kernel, double* total_ms, int64_t* launches);
+cf_status cf_context_reset_timing(cf_context* ctx);
+/* Number of kernel launches issued by this context since creation. */
+int64_t cf_context_launch_count(cf_context* ctx);
+
+/* ---------------------------------------------------------------------------------------------
+ * Datasets: integral images resident in device memory
+ * Replaces RGBDImage::calculateIntegral (image.cpp:531-556) and ImageCache (random_tree_image_gpu.cu:727-908).
+ * ------------------------------------------------------------------------------------------- */
+cf_status cf_dataset_create(cf_context* ctx, int num_images, int width, int height, cf_dataset** out);
+cf_status cf_dataset_destroy(cf_dataset* ds);
+/* Raw frames -> integral images on the GPU. rgb uint8 [count][H][W][3], depth_mm uint16 [count][H][W]
+ * (0 = missing). `device_pointers` != 0 means both inputs already live in device memory. */
+cf_status cf_dataset_upload_raw(cf_dataset* ds, int first, int count, const uint8_t* rgb,
+                                const uint16_t* depth_mm, int device_pointers);
+/* Already-integrated images in the reference layout: colour float [count][3][H][W], depth int32
+ * [count][2][H][W] (sum in mm, valid count), e.g. from RGBDImage::getColorImage/getDepthImage. */
+cf_status cf_dataset_upload_integral(cf_dataset* ds, int first, int count, const float* color,
+                                     const int32_t* depth);
+cf_status cf_dataset_download_integral(cf_dataset* ds, int first, int count, float* color, int32_t* depth);
+cf_status cf_dataset_info(cf_dataset* ds, int* num_images, int* width, int* height);
+
+/* ---------------------------------------------------------------------------------------------
+ * ImageFeatureEvaluation (random_tree_image.h:988-1096), host buffers
+ * Features are the int8 [11][F] table of ImageFeaturesAndThresholds (random_tree_image.h:635-912):
+ * rows type, offset1X, offset1Y, offset2X, offset2Y, region1X, region1Y, region2X, region2Y,
+ * channel1, channel2. Thresholds are float [T][F].
+ * ------------------------------------------------------------------------------------------- */
+/* featureResponseKernel (random_tree_image_gpu.cu:1455-1545): responses double [F][N]. */
+cf_status cf_feature_responses(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_features,
+                               const int8_t* features, double* responses);
+/* calculateFeatureResponsesAndHistograms (random_tree_image_gpu.cu:1958-2135): counters uint32
+ * [F][T][C][2] (0 = left, 1 = right), exact for any number of classes <= 256. */
+cf_status cf_histograms(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_features,
+                        int num_thresholds, const int8_t* features, const float* thresholds, int num_classes,
+                        uint32_t* counters);
+/* calculateScores (random_tree_image_gpu.cu:2137-2182): scores double [T][F] from counters
+ * [F][T][C][2] and the node histogram [C]. */
+cf_status cf_scores(cf_context* ctx, int num_classes, int num_features, int num_thresholds,
+                    const uint32_t* counters, const uint32_t* node_histogram, double* scores);
+/* generateRandomFeatures (random_tree_image_gpu.cu:1896-1956 + sortFeatures :1853-1894): the
+ * candidate generator of the GPU path on a Philox4x32-10 stream, sorted by getSortKey. */
+cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample* samples, uint32_t seed,
+                               int num_features, int num_thresholds, int box_radius, int region_size,
+                               int use_depth_images, int8_t* features, float* thresholds);
+/* evaluateBestSplits (random_tree_image.cpp:239-502) for all open nodes of one level in one
+ * persistent launch. Node n owns samples [node_offsets[n], node_offsets[n+1]). */
+cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* node_offsets,
+                                  const cf_sample* samples, int num_classes, int num_features,
+                                  int num_thresholds, const int8_t* features, const float* thresholds,
+                                  cf_split* best);
+
+/* ---------------------------------------------------------------------------------------------
+ * Tree training
+ * ------------------------------------------------------------------------------------------- */
+#define CF_TRAIN_LEVEL_BATCHED 0   /* all open nodes of a level in one persistent launch */
+#define CF_TRAIN_PER_NODE 1        /* reference structure: per node responses -> histograms -> scores -> host argmax */
+
+/* RandomTreeImage::train from a sample list (random_tree_image.cpp:746-824 after sampling) driving
+ * RandomTreeTrain::train (random_tree.h:1249-1415). The level seeds are drawn from the tree's
+ * RandomSource starting at *seed_counter, which is advanced as the reference advances it. */
+cf_status cf_train_tree(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                        const cf_train_config* config, int tree_id, int32_t* seed_counter, int mode,
+                        cf_tree** out);
+/* RandomForestImage::train (random_forest_image.cpp:132-182) on raw host frames: GPU integral images,
+ * class-uniform sampling (random_tree_image.cpp:911-1059, one host thread), block sort, then
+ * cf_train_tree per tree. labels uint8 [n][H][W]; ignored[C] marks ignoredColors. */
+cf_status cf_forest_train(cf_context* ctx, int num_images, int width, int height, const uint8_t* rgb,
+                          const uint16_t* depth_mm, const uint8_t* labels, int num_classes,
+                          const uint8_t* ignored, const cf_train_config* config, int num_trees, int mode,
+                          cf_tree** trees);
+/* The forest seed of RandomForestImage::train (random_forest_image.cpp:150-151): the first draw of
+ * uniformSampler(0xFFFF) on RandomSource(random_seed). Tree t uses seed counter SEED + t. */
+cf_status cf_forest_seed(int32_t random_seed, int32_t* seed);
+/* Training pixels of one tree as RandomForestImage::train draws them (maxImages reservoir
+ * random_forest_image.cpp:161-171, class prior random_tree_image.cpp:885-909, class- or
+ * pixel-uniform sampling :840-1059 on one host thread, block sort :776-802). *seed_counter is the
+ * tree's RandomSource counter and is advanced; prior[C] receives the class prior (may be NULL).
+ * With out == NULL only *count is set. */
+cf_status cf_sample_tree_pixels(int num_images, int width, int height, const uint8_t* labels,
+                                const uint16_t* depth_mm, int num_classes, const uint8_t* ignored,
+                                const cf_train_config* config, int num_trees, int32_t* seed_counter,
+                                cf_sample* out, int64_t capacity, int64_t* count, uint32_t* prior);
+/* RandomTree accessors (random_tree.h:499-1003). */
+cf_status cf_tree_info(cf_tree* tree, int* num_nodes, int* num_classes, int* depth, int* tree_id);
+/* Node arrays in breadth-first id order (index = nodeId - treeId); any pointer may be NULL.
+ * level, left (-1 leaf; right child = left + 1), feature int8 [n][11], threshold, score, feature_id,
+ * histogram uint32 [n][C], num_samples. */
+cf_status cf_tree_export(cf_tree* tree, int32_t* level, int32_t* left, int8_t* feature, float* threshold,
+                         double* score, int32_t* feature_id, uint32_t* histogram, uint32_t* num_samples);
+cf_status cf_tree_import(int tree_id, int num_nodes, int num_classes, const int32_t* level, const int32_t* left,
+                         const int8_t* feature, const float* threshold, const double* score,
+                         const int32_t* feature_id, const uint32_t* histogram, cf_tree** out);
+cf_status cf_tree_destroy(cf_tree* tree);
+/* classLabelPriorDistribution of the tree (RandomTreeImage::getClassLabelPriorDistribution,
+ * random_tree_image.h:1160-1163): pixel counts per class over its training images. */
+cf_status cf_tree_prior(cf_tree* tree, uint32_t* prior, int capacity, int* count);
+cf_status cf_tree_set_prior(cf_tree* tree, const uint32_t* prior, int count);
+/* Per-level statistics of the last training of this tree: feature evaluations and device time. */
+cf_status cf_tree_train_stats(cf_tree* tree, int64_t* feature_evals, double* device_ms, int* levels);
+
+/* ---------------------------------------------------------------------------------------------
+ * Prediction: RandomForestImage::normalizeHistograms + convertTree + predict
+ * (random_forest_image.cpp:258-376; random_tree_image_gpu.cu:424-578, 1237-1453)
+ * ------------------------------------------------------------------------------------------- */
+/* Normalises every leaf histogram (detail::normalizeHistogram, random_tree.cpp:54-104) with the
+ * class prior [C] (NULL: each tree's own prior) and packs the trees for the traversal kernel. */
+cf_status cf_forest_create(cf_context* ctx, int num_trees, cf_tree* const* trees, const uint32_t* prior,
+                           double histogram_bias, int use_labels_prior, cf_forest** out);
+cf_status cf_forest_destroy(cf_forest* forest);
+cf_status cf_forest_info(cf_forest* forest, int* num_trees, int* num_classes, int64_t* num_nodes);
+/* Dense prediction of `count` dataset images from `first`: probabilities float [count][C][H][W] and
+ * labels uint8 [count][H][W], both DEVICE pointers (either may be NULL). */
+cf_status cf_predict_dataset(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
+                             uint8_t* labels);
+/* Same from raw host frames, results to host buffers (either may be NULL). */
+cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, const uint8_t* rgb,
+                          const uint16_t* depth_mm, float* probabilities, uint8_t* labels);
+
+/* ---------------------------------------------------------------------------------------------
+ * Serving: continuous batching of mixed-resolution frames on a resident forest
+ * (replaces the per-image test() loop, predict.cpp:209-375)
+ * ------------------------------------------------------------------------------------------- */
+typedef struct cf_server_config {
+    int64_t hbm_budget_bytes;   /* admission limit for frames in flight */
+    int32_t max_batch_frames;   /* frames per launch */
+    int32_t max_pending;        /* queue length before submits are rejected */
+    int32_t pipeline_depth;     /* batches in flight on the device */
+    int32_t return_probabilities;
+} cf_server_config;
+
+typedef struct cf_request_stats {
+    double submit_ms;      /* host clock at submit, ms since server start */
+    double admitted_ms;
+    double done_ms;
+    int32_t batch_id;
+    int32_t batch_frames;
+} cf_request_stats;
+
+cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf_server** out);
+cf_status cf_server_destroy(cf_server* server);
+/* Copies the frame; returns at once with a request id. */
+cf_status cf_server_submit(cf_server* server, int width, int height, const uint8_t* rgb, const uint16_t* depth_mm,
+                           int64_t* request_id);
+/* Waits (bounded) for a request; copies labels uint8 [H][W] and, if the server returns them,
+ * probabilities float [C][H][W] (either pointer may be NULL). */
+cf_status cf_server_wait(cf_server* server, int64_t request_id, double timeout_s, uint8_t* labels,
+                         float* probabilities, cf_request_stats* stats);
+cf_status cf_server_counters(cf_server* server, int64_t* submitted, int64_t* completed, int64_t* rejected,
+                             int64_t* batches);
+
+/* ---------------------------------------------------------------------------------------------
+ * Tree files: gzip-compressed JSON (RandomTreeExport::writeJSON export.cpp:292-313,
+ * RandomTreeImport::readJSON import.cpp:175-266)
+ * ------------------------------------------------------------------------------------------- */
+cf_status cf_tree_write_json(cf_tree* tree, const cf_train_config* config, const uint32_t* prior,
+                             const char* path, int verbose);
+cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t* prior, int prior_capacity,
+                            cf_tree** out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Synthetic RGB-D frames (seeded Voronoi scenes) for tests and benchmarks
+ * ------------------------------------------------------------------------------------------- */
+cf_status cf_synthetic_frames(uint64_t seed, int num_images, int width, int height, int num_cells,
+                              int num_classes, int void_class, uint8_t* rgb, uint16_t* depth_mm,
+                              uint8_t* labels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -498,10 +498,13 @@ void orc_generate_features(const orc_dataset* ds, int num_samples, const orc_sam
         int8_t o1x, o1y, o2x, o2y, r1x, r1y, r2x, r2y;
         offset(&o1x, &o1y);
         region(&r1x, &r1y);
+        /* redraw bounded at 1000 tries, then the x offset moves by one (same rule as the kernel) */
+        int redraws = 0;
         do {
             offset(&o2x, &o2y);
             region(&r2x, &r2y);
-        } while (o1x == o2x && o1y == o2y);
+        } while (o1x == o2x && o1y == o2y && ++redraws < 1000);
+        if (o1x == o2x && o1y == o2y) o2x = static_cast<int8_t>(o1x + 1);
         uint8_t ch1 = 0, ch2 = 0;
         if (type == 1) {
             if (use_depth_images) {

@@ -1,0 +1,151 @@
+"""CPU-only checks of the C-ABI library: it loads, exports every declared entry point, reports
+errors as status codes, and its host-only parts (tree import/export, JSON files, synthetic frames)
+work without a GPU."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import curfil_b200 as cf
+from curfil_b200 import _build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built_library():
+    _build.build()
+    yield
+
+
+def declared_functions():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names.update(re.findall(r"\b(cf_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = cf.lib()
+    names = declared_functions()
+    assert len(names) > 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, "not exported: %s" % missing
+
+
+def test_version_string():
+    assert "sm_100a" in cf.version()
+
+
+def test_errors_are_status_codes_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-device path")
+    with pytest.raises(cf.CurfilError) as e:
+        cf.Context(0)
+    assert e.value.status in (1, 2)
+
+
+def test_synthetic_frames_deterministic():
+    a = cf.synthetic_frames(7, 3, 64, 48, 12, 8)
+    b = cf.synthetic_frames(7, 3, 64, 48, 12, 8)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    rgb, depth, labels = a
+    assert rgb.shape == (3, 48, 64, 3) and depth.shape == (3, 48, 64)
+    assert labels.max() < 8
+    holes = (depth == 0).mean()
+    assert 0.05 < holes < 0.15
+    assert depth[depth > 0].min() >= 500 and depth.max() <= 5000
+
+
+def small_tree(C=3):
+    # n0 -> (n1, n2); n1 -> (n3, n4)   (random_tree_image_gpu_test.cu:990-1130)
+    left = np.array([1, 3, -1, -1, -1], np.int32)
+    feature = np.zeros((5, 11), np.int8)
+    feature[0] = [0, -18, 25, 9, 28, 4, 19, 1, 16, 0, 0]
+    feature[1] = [1, -10, 5, 27, -19, 7, 3, 65, 73, 1, 2]
+    threshold = np.array([-29.1245, 28.391, np.nan, np.nan, np.nan], np.float32)
+    hist = np.array([[70, 60, 30], [10, 10, 10], [60, 60, 20], [10, 0, 20], [0, 50, 20]], np.uint32)
+    score = np.array([0.9371, 0.392, np.nan, np.nan, np.nan])
+    fid = np.array([2, 1, -1, -1, -1], np.int32)
+    return cf.Tree.from_arrays(0, left, feature, threshold, hist, score=score, feature_id=fid)
+
+
+def test_tree_import_export_roundtrip():
+    t = small_tree()
+    a = t.arrays()
+    assert t.num_nodes == 5 and t.depth == 3
+    np.testing.assert_array_equal(a["level"], [1, 2, 2, 3, 3])
+    np.testing.assert_array_equal(a["left"], [1, 3, -1, -1, -1])
+    assert a["threshold"][0] == np.float32(-29.1245)
+
+
+def test_tree_json_roundtrip(tmp_path):
+    t = small_tree()
+    t.set_prior([100, 100, 100])
+    cfg = cf.TrainConfig(feature_count=1000, thresholds=50, max_depth=15, box_radius=127, region_size=50)
+    path = tmp_path / "tree0.json.gz"
+    t.write_json(path, cfg)
+    t2, cfg2, prior2 = cf.Tree.read_json(path)
+    a, b = t.arrays(), t2.arrays()
+    for k in ("level", "left", "feature", "feature_id", "histogram"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    np.testing.assert_array_equal(a["threshold"][a["left"] >= 0], b["threshold"][b["left"] >= 0])
+    np.testing.assert_array_equal(a["score"][a["left"] >= 0], b["score"][b["left"] >= 0])
+    np.testing.assert_array_equal(prior2, [100, 100, 100])
+    assert (cfg2.feature_count, cfg2.thresholds, cfg2.max_depth, cfg2.box_radius, cfg2.region_size) == \
+        (1000, 50, 15, 127, 50)
+    # file is gzip JSON with string values, as boost::property_tree writes it
+    import gzip
+    import json
+    doc = json.loads(gzip.open(path).read().decode())
+    assert doc["tree"]["split"]["featureId"] == "2"
+    assert doc["tree"]["left"]["split"]["feature"]["type"] == "color"
+    assert doc["tree"]["split"]["feature"]["offset1"] == ["-18", "25"]
+    assert "deviceId" in doc and doc["classLabelPriorDistribution"]["1"] == "100"
+
+
+def test_tree_json_rejects_corrupt_files(tmp_path):
+    p = tmp_path / "bad.json.gz"
+    import gzip
+    with gzip.open(p, "wb") as f:
+        f.write(b'{"tree": {"id": "0"')
+    with pytest.raises(cf.CurfilError) as e:
+        cf.Tree.read_json(p)
+    assert e.value.status == 8
+    with pytest.raises(cf.CurfilError):
+        cf.Tree.read_json(tmp_path / "missing.json.gz")
+
+
+def test_tree_import_rejects_bad_child_index():
+    left = np.array([5, -1, -1], np.int32)
+    with pytest.raises(cf.CurfilError) as e:
+        cf.Tree.from_arrays(0, left, np.zeros((3, 11), np.int8), np.zeros(3, np.float32),
+                            np.ones((3, 2), np.uint32))
+    assert e.value.status == 1
+
+
+def test_tree_sampling_matches_oracle():
+    """cf_sample_tree_pixels (product) vs the oracle restatement of class-uniform sampling."""
+    from oracle import pyoracle as orc
+    rgb, depth, labels = cf.synthetic_frames(4, 3, 64, 48, 10, 8)
+    cfg = cf.TrainConfig(samples_per_image=300)
+    seed = cf.forest_seed(4711)
+    assert seed == int(orc.sampler_draws(4711, 0, 0xFFFE, 1)[0])
+    ignore = np.zeros(8, np.uint8)
+    ignore[0] = 1
+    for t in range(2):
+        s, prior, counter = cf.sample_tree_pixels(labels, depth, 8, cfg, 2, seed + t, ignored=ignore)
+        rc, o, ocounter = orc.sample_class_uniform(labels, depth, 8, ignore, 150, seed + t)
+        assert rc == len(s) and counter == ocounter
+        for k in ("x", "y", "image", "label", "flip"):
+            np.testing.assert_array_equal(s[k], o[k], err_msg=k)
+        np.testing.assert_array_equal(s["depth"].view(np.uint32), o["depth"].view(np.uint32))
+        np.testing.assert_array_equal(prior, np.bincount(labels.ravel(), minlength=8))
+        assert (s["label"] != 0).all()

@@ -1,0 +1,85 @@
+"""Serving: continuous batching of mixed-size frames; every result is the same alone and in the mix."""
+import numpy as np
+import pytest
+
+import curfil_b200 as cf
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def forest():
+    from curfil_b200 import _build
+    _build.build()
+    ctx = cf.Context(0)
+    rgb, depth, labels = H.frames(seed=12, n=3, w=96, h=72, cells=12, classes=10)
+    ds = cf.Dataset.from_raw(ctx, rgb, depth)
+    trees = []
+    for t in range(3):
+        samples, _ = H.class_uniform_samples(labels, depth, 10, 40, seed_counter=300 + 7 * t)
+        cfg = cf.TrainConfig(feature_count=100, thresholds=10, max_depth=9, min_sample_count=4, box_radius=40,
+                             region_size=10)
+        tree, _ = cf.train_tree(ds, samples, 10, cfg, tree_id=t, seed_counter=11 * t + 1)
+        tree.set_prior(np.bincount(labels.ravel(), minlength=10))
+        trees.append(tree)
+    f = cf.Forest(ctx, trees)
+    yield f
+    f.close()
+    ctx.close()
+
+
+SIZES = [(160, 120), (320, 240), (640, 480), (1280, 960)]
+
+
+def test_alone_and_in_mix_identical(forest):
+    server = cf.Server(forest, hbm_budget_bytes=2 << 30, max_batch_frames=8, pipeline_depth=2,
+                       return_probabilities=True)
+    frames = {}
+    for k, (w, h) in enumerate(SIZES):
+        rgb, depth, _ = cf.synthetic_frames(500 + k, 1, w, h, 12, 10)
+        frames[(w, h)] = (rgb[0], depth[0])
+    # alone
+    alone = {}
+    for key, (rgb, depth) in frames.items():
+        rid = server.submit(rgb, depth)
+        alone[key] = server.wait(rid, depth.shape, probabilities=True)
+    # mixed burst: 1:2:4:1 of the four sizes, submitted back to back
+    order = [SIZES[0]] + [SIZES[1]] * 2 + [SIZES[2]] * 4 + [SIZES[3]]
+    rng = np.random.default_rng(3)
+    rng.shuffle(order)
+    ids = [(key, server.submit(*frames[key])) for key in order for _ in range(2)]
+    mixed_batches = set()
+    for key, rid in ids:
+        labels, probs, st = server.wait(rid, frames[key][1].shape, probabilities=True)
+        np.testing.assert_array_equal(labels, alone[key][0])
+        np.testing.assert_array_equal(probs, alone[key][1])
+        if st.batch_frames > 1:
+            mixed_batches.add(st.batch_id)
+        assert st.done_ms >= st.admitted_ms >= st.submit_ms
+    c = server.counters()
+    assert c["completed"] == c["submitted"] == len(ids) + len(SIZES)
+    assert mixed_batches, "no batch held more than one frame"
+    assert c["batches"] < c["submitted"]
+    # and the same as the direct prediction path
+    for key, (rgb, depth) in frames.items():
+        probs, labels = forest.predict(rgb, depth)
+        np.testing.assert_array_equal(labels[0], alone[key][0])
+        np.testing.assert_array_equal(probs[0], alone[key][1])
+    server.close()
+
+
+def test_admission_rejects_oversized_and_unknown(forest):
+    server = cf.Server(forest, hbm_budget_bytes=8 << 20, max_batch_frames=4, pipeline_depth=2)
+    rgb, depth, _ = cf.synthetic_frames(1, 1, 1280, 960, 12, 10)
+    with pytest.raises(cf.CurfilError) as e:
+        server.submit(rgb[0], depth[0])
+    assert e.value.status == 7
+    small_rgb, small_depth, _ = cf.synthetic_frames(2, 1, 160, 120, 12, 10)
+    rid = server.submit(small_rgb[0], small_depth[0])
+    labels, _, _ = server.wait(rid, (120, 160))
+    assert labels.shape == (120, 160)
+    with pytest.raises(cf.CurfilError):
+        server.wait(123456789, (1, 1), timeout_s=0.01)
+    assert server.counters()["rejected"] == 1
+    server.close()
