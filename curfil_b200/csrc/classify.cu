@@ -266,6 +266,7 @@ cf_status cf_forest_create(cf_context* ctx, int num_trees, cf_tree* const* trees
         CF_CUDA_CHECK(cudaMemcpyAsync(f->leaves.get(), leaves.data(), sizeof(float) * leaves.size(),
                                       cudaMemcpyHostToDevice, ctx->stream));
         CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+        context_retain(ctx);
         *out = guard_f.release();
     });
 }
@@ -273,9 +274,11 @@ cf_status cf_forest_create(cf_context* ctx, int num_trees, cf_tree* const* trees
 cf_status cf_forest_destroy(cf_forest* forest) {
     return guard([&] {
         if (!forest) return;
-        cudaSetDevice(forest->ctx->device);
-        cudaStreamSynchronize(forest->ctx->stream);
+        cf_context* ctx = forest->ctx;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
         delete forest;
+        context_release(ctx);
     });
 }
 

@@ -11,6 +11,25 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+void destroy_context_now(cf_context* ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->kernel_events)
+        for (auto& pr : kv.second.pending) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+void context_retain(cf_context* ctx) { ctx->refs++; }
+
+void context_release(cf_context* ctx) {
+    if (--ctx->refs == 0 && ctx->closed.load()) destroy_context_now(ctx);
+}
+
 LaunchScope::LaunchScope(cf_context* ctx, cudaStream_t stream, const char* name)
     : ctx_(ctx), stream_(stream), name_(name) {
     if (ctx_->timing) {
@@ -97,16 +116,8 @@ cf_status cf_context_create(int device, cf_context** out) {
 cf_status cf_context_destroy(cf_context* ctx) {
     return cf::guard([&] {
         if (!ctx) return;
-        cudaSetDevice(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
-        for (auto& kv : ctx->kernel_events)
-            for (auto& pr : kv.second.pending) {
-                cudaEventDestroy(pr.first);
-                cudaEventDestroy(pr.second);
-            }
-        for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
-        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
-        delete ctx;
+        ctx->closed = true;
+        if (ctx->refs.load() == 0) cf::destroy_context_now(ctx);
     });
 }
 

@@ -164,6 +164,7 @@ cf_status cf_dataset_create(cf_context* ctx, int num_images, int width, int heig
             delete ds;
             throw;
         }
+        cf::context_retain(ctx);
         *out = ds;
     });
 }
@@ -171,9 +172,11 @@ cf_status cf_dataset_create(cf_context* ctx, int num_images, int width, int heig
 cf_status cf_dataset_destroy(cf_dataset* ds) {
     return cf::guard([&] {
         if (!ds) return;
-        cudaSetDevice(ds->ctx->device);
-        cudaStreamSynchronize(ds->ctx->stream);
+        cf_context* ctx = ds->ctx;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
         delete ds;
+        cf::context_release(ctx);
     });
 }
 

@@ -139,6 +139,9 @@ struct cf_context {
     cudaStream_t stream = nullptr;
     bool timing = false;
     std::atomic<int64_t> launches{0};
+    // objects (datasets, forests, servers) holding this context; destruction waits for the last
+    std::atomic<int> refs{0};
+    std::atomic<bool> closed{false};
     std::mutex mu;
     struct KernelEvents {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
@@ -184,6 +187,10 @@ inline void launch(cf_context* ctx, const char* name, dim3 grid, dim3 block, siz
 }
 
 inline void make_current(cf_context* ctx) { CF_CUDA_CHECK(cudaSetDevice(ctx->device)); }
+
+// A closed context is freed when the last object using it is destroyed.
+void context_retain(cf_context* ctx);
+void context_release(cf_context* ctx);
 
 }  // namespace cf
 

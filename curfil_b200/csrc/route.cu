@@ -285,7 +285,7 @@ void Scanner::exclusive(cf_context* ctx, const uint32_t* in, uint32_t* out, long
 void Scanner::scan_level(cf_context* ctx, const uint32_t* in, uint32_t* out, long long n_in, long long n_out,
                          size_t depth) {
     const long long tiles = (n_out + kScanTile - 1) / kScanTile;
-    if (temps_.size() < 2 * (depth + 1)) temps_.resize(2 * (depth + 1));
+    CF_REQUIRE(depth < kMaxDepth, "scan: input too large");
     DevArray<uint32_t>& sums = temps_[2 * depth];
     DevArray<uint32_t>& offsets = temps_[2 * depth + 1];
     sums.reserve(tiles + 1);

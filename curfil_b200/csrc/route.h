@@ -25,7 +25,10 @@ public:
 
 private:
     void scan_level(cf_context* ctx, const uint32_t* in, uint32_t* out, long long n_in, long long n_out, size_t depth);
-    std::vector<DevArray<uint32_t>> temps_;
+    // two buffers per recursion depth; a fixed array so references stay valid while recursing
+    // (1024^8 elements is far beyond any sample count)
+    static constexpr size_t kMaxDepth = 8;
+    DevArray<uint32_t> temps_[2 * kMaxDepth];
 };
 
 struct RouteBuffers {

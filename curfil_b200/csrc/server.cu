@@ -305,6 +305,7 @@ cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf
         cf_server* raw = s.get();
         s->launcher = std::thread([raw] { raw->launch_loop(); });
         s->completer = std::thread([raw] { raw->complete_loop(); });
+        context_retain(ctx);
         *out = s.release();
     });
 }
@@ -341,7 +342,9 @@ cf_status cf_server_destroy(cf_server* server) {
             }
             if (s->done) cudaEventDestroy(s->done);
         }
+        cf_context* ctx = server->ctx;
         delete server;
+        context_release(ctx);
     });
 }
 

@@ -56,8 +56,10 @@ def test_integral_1280x960_box_sums_exact_beyond_int32(ctx):
     depth = np.full((1, h, w), 5000, np.uint16)
     ds = cf.Dataset.from_raw(ctx, rgb, depth)
     color, dint = ds.download_integral()
-    s = dint[0, 0].astype(np.int64).view(np.uint64) if False else dint[0, 0].view(np.uint32).astype(np.int64)
-    for (x0, y0, x1, y1) in [(0, 0, 1279, 959), (100, 200, 160, 260), (1200, 900, 1279, 959)]:
+    s = dint[0, 0].view(np.uint32).astype(np.int64)
+    # the whole-frame sum (6.1e9) wraps; every box a feature can reach (< 2^31 mm) is exact
+    assert s[h - 1, w - 1] == (h * w * 5000) % (1 << 32)
+    for (x0, y0, x1, y1) in [(100, 200, 160, 260), (1200, 900, 1279, 959), (0, 0, 300, 280)]:
         box = ((s[y1, x1] - s[y0, x1]) + (s[y0, x0] - s[y1, x0])) % (1 << 32)
         assert box == (x1 - x0) * (y1 - y0) * 5000
     assert color[0, 0, h - 1, w - 1] == np.float32(255.0 * h * w)
