@@ -203,7 +203,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    # workload size (defaults: the full-size configuration); smaller cases are for profiler captures
+    ap.add_argument("--images", type=int, default=W["images"])
+    ap.add_argument("--trees", type=int, default=W["trees"])
+    ap.add_argument("--max-depth", type=int, default=W["max_depth"])
+    ap.add_argument("--predict-images", type=int, default=W["predict_images"])
     args = ap.parse_args()
+    W.update(images=args.images, trees=args.trees, max_depth=args.max_depth,
+             predict_images=min(args.predict_images, args.images))
     if args.impl == "reference":
         run_reference(args)
         return
@@ -298,23 +305,26 @@ def main():
                 traffic = float(ln.split(":")[1]) * total_evals / max(1, eval_launches)
 
     # prediction of 50 resident frames with the trained forest
-    forest = cf.Forest(ctx, trees)
     n_pred = W["predict_images"]
-    probs = torch.empty((n_pred, W["classes"], W["height"], W["width"]), dtype=torch.float32, device=local)
-    lab = torch.empty((n_pred, W["height"], W["width"]), dtype=torch.uint8, device=local)
-    with torch.cuda.stream(stream):
-        forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
-        pstart, pend = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        pstart.record(stream)
-        reps = 3
-        for _ in range(reps):
+    predict = None
+    if n_pred > 0:
+        forest = cf.Forest(ctx, trees)
+        probs = torch.empty((n_pred, W["classes"], W["height"], W["width"]), dtype=torch.float32, device=local)
+        lab = torch.empty((n_pred, W["height"], W["width"]), dtype=torch.uint8, device=local)
+        with torch.cuda.stream(stream):
             forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
-        pend.record(stream)
-        torch.cuda.synchronize()
-    pred_ms = pstart.elapsed_time(pend) / reps
-    mpx = n_pred * W["width"] * W["height"] / (pred_ms / 1e3) / 1e6
-    forest.close()
+            pstart, pend = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            pstart.record(stream)
+            reps = 3
+            for _ in range(reps):
+                forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
+            pend.record(stream)
+            torch.cuda.synchronize()
+        pred_ms = pstart.elapsed_time(pend) / reps
+        predict = {"images": n_pred, "mpx_per_s": n_pred * W["width"] * W["height"] / (pred_ms / 1e3) / 1e6,
+                   "ms_per_batch": pred_ms, "ms_per_frame": pred_ms / n_pred, "trees": W["trees"]}
+        forest.close()
 
     # end to end through cf_forest_train with host buffers
     e2e = None
@@ -352,8 +362,7 @@ def main():
                 "kernel_ms": kernel_ms,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks.summary(),
-                "predict": {"images": n_pred, "mpx_per_s": mpx, "ms_per_batch": pred_ms,
-                            "ms_per_frame": pred_ms / n_pred, "trees": W["trees"]},
+                "predict": predict,
                 "feature_evals_per_step": total_evals / args.steps}
         print(json.dumps(line), flush=True)
     ds.close()
