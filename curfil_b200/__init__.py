@@ -263,6 +263,18 @@ def evaluate_best_splits(ds, node_offsets, samples, num_classes, features, thres
     return out
 
 
+def evaluate_best_splits_noalloc(ctx, color_ptr, depth_ptr, num_images, width, height, node_offsets, samples_ptr,
+                                 node_hist_ptr, num_classes, num_features, num_thresholds, features_ptr,
+                                 thresholds_ptr, best_ptr):
+    """cf_evaluate_best_splits without device allocation: every array argument except the host
+    `node_offsets` is a device pointer owned by the caller (see include/curfil_b200.h)."""
+    node_offsets = np.ascontiguousarray(node_offsets, np.int64)
+    _check(lib().cf_evaluate_best_splits_noalloc(
+        ctx.handle, _vp(color_ptr), _vp(depth_ptr), int(num_images), int(width), int(height),
+        len(node_offsets) - 1, _p(node_offsets), _vp(samples_ptr), _vp(node_hist_ptr), int(num_classes),
+        int(num_features), int(num_thresholds), _vp(features_ptr), _vp(thresholds_ptr), _vp(best_ptr)))
+
+
 class Tree:
     """cf_tree: a trained tree in breadth-first node arrays (index = nodeId - treeId)."""
 

@@ -638,3 +638,193 @@ void PlainNodeEvaluator::evaluate_node(cf_context* ctx, const DsView& ds, const 
 }
 
 }  // namespace cf
+
+// ================================================================================================
+// Allocation-free variant of the level-batched split search
+// ================================================================================================
+//
+// Some callers cannot let a library allocate device memory: a host that owns all GPU memory
+// through its own pool and hands out fixed buffers, or a latency-critical loop where cudaMalloc /
+// cudaFree would synchronise the device and stall its other streams. For them this entry point
+// takes every input and output as a device pointer and keeps its scratch (work items, candidate
+// lists, node descriptors, prepared feature tables) in one fixed device array compiled into the
+// library.
+namespace cf {
+
+__global__ void prepare_eval_features_kernel(int F, int T, const int8_t* __restrict__ feat,
+                                             const float* __restrict__ thr, FeatParams* __restrict__ packs,
+                                             float* __restrict__ sorted_thr, uint16_t* __restrict__ ranks);
+
+namespace {
+
+// 16 MiB per device, held by every GPU that loads the library until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+constexpr int kNoAllocMaxNodes = 65536;
+constexpr int kNoAllocMaxItems = 65536;
+constexpr long long kNoAllocMaxFeatureThresholds = 1LL << 20;  // features x thresholds
+constexpr int kNoAllocMaxFeatures = 16384;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocLayout {
+    size_t nodes, items, order, range, cands, queue, packs, sorted, ranks, total;
+    NoAllocLayout(int M, int n_items, int F, int T) {
+        auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
+        size_t o = 0;
+        nodes = o;
+        o += a(sizeof(NodeDesc) * M);
+        items = o;
+        o += a(sizeof(EvalItem) * n_items);
+        order = o;
+        o += a(sizeof(int) * n_items);
+        range = o;
+        o += a(sizeof(int) * (M + 1));
+        cands = o;
+        o += a(sizeof(ItemCandidates) * n_items);
+        queue = o;
+        o += a(sizeof(int));
+        packs = o;
+        o += a(sizeof(FeatParams) * F);
+        sorted = o;
+        o += a(sizeof(float) * static_cast<size_t>(F) * T);
+        ranks = o;
+        o += a(sizeof(uint16_t) * static_cast<size_t>(F) * T);
+        total = o;
+    }
+};
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[128] = {};
+
+// Device address of the scratch array on `device` (the current device). Host code cannot use the
+// array's name as a device address, so it is looked up once per device and cached.
+char* noalloc_scratch(int device) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    CF_REQUIRE(device >= 0 && device < 128, "allocation-free split search: device index out of range");
+    if (g_noalloc_addr[device] == nullptr) {
+        void* p = nullptr;
+        CF_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[device] = p;
+    }
+    return static_cast<char*>(g_noalloc_addr[device]);
+}
+
+}  // namespace
+}  // namespace cf
+
+extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const float* color, const int32_t* depth,
+                                                     int num_images, int width, int height, int num_nodes,
+                                                     const int64_t* node_offsets, const cf_sample* samples,
+                                                     const uint32_t* node_histograms, int num_classes,
+                                                     int num_features, int num_thresholds, const int8_t* features,
+                                                     const float* thresholds, cf_split* best) {
+    using namespace cf;
+    return guard([&] {
+        CF_REQUIRE(ctx && color && depth && node_offsets && samples && node_histograms && features && thresholds &&
+                       best,
+                   "cf_evaluate_best_splits_noalloc: NULL argument");
+        CF_REQUIRE(num_images >= 1 && width >= 1 && height >= 1, "cf_evaluate_best_splits_noalloc: empty images");
+        CF_REQUIRE(num_nodes >= 1 && num_nodes <= kNoAllocMaxNodes,
+                   "cf_evaluate_best_splits_noalloc: num_nodes must be in [1, 65536]");
+        CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_evaluate_best_splits_noalloc: classes must be in [1, 256]");
+        CF_REQUIRE(num_features >= 1 && num_features <= kNoAllocMaxFeatures && num_thresholds >= 1 &&
+                       static_cast<long long>(num_features) * num_thresholds <= kNoAllocMaxFeatureThresholds,
+                   "cf_evaluate_best_splits_noalloc: features x thresholds beyond the fixed scratch "
+                   "(at most 16384 features and 2^20 feature-threshold pairs)");
+        CF_REQUIRE(node_offsets[0] == 0, "cf_evaluate_best_splits_noalloc: node offsets must start at 0");
+        make_current(ctx);
+        const int M = num_nodes, F = num_features, T = num_thresholds, C = num_classes;
+        // nodes and work items, sized as the level-batched evaluator sizes them
+        std::vector<NodeDesc> nodes(M);
+        long long total_work = 0;
+        for (int i = 0; i < M; i++) {
+            const long long cnt = node_offsets[i + 1] - node_offsets[i];
+            CF_REQUIRE(cnt >= 1 && cnt < (1LL << 31), "cf_evaluate_best_splits_noalloc: every node needs samples");
+            nodes[i] = NodeDesc{node_offsets[i], static_cast<int>(cnt), i};
+            total_work += cnt * F;
+        }
+        const EvalTuning tuning;
+        const int slots = ctx->num_sms * tuning.ctas_per_sm;
+        const double work_per_item = std::max(1.0, static_cast<double>(total_work) / (tuning.items_per_slot * slots));
+        std::vector<EvalItem> items;
+        std::vector<int> range(M + 1);
+        std::vector<long long> work;
+        for (int n = 0; n < M; n++) {
+            range[n] = static_cast<int>(items.size());
+            int parts = static_cast<int>(std::ceil(static_cast<double>(nodes[n].count) * F / work_per_item));
+            parts = std::max(1, std::min(parts, (F + 7) / 8));
+            int per = (F + parts - 1) / parts;
+            per = ((per + 7) / 8) * 8;
+            for (int f0 = 0; f0 < F; f0 += per) {
+                items.push_back(EvalItem{n, f0, std::min(F, f0 + per), 0});
+                work.push_back(static_cast<long long>(nodes[n].count) * (std::min(F, f0 + per) - f0));
+            }
+            CF_REQUIRE(static_cast<int>(items.size()) <= kNoAllocMaxItems,
+                       "cf_evaluate_best_splits_noalloc: level needs more than 65536 work items");
+        }
+        range[M] = static_cast<int>(items.size());
+        const int n_items = static_cast<int>(items.size());
+        std::vector<int> order(n_items);
+        for (int i = 0; i < n_items; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+
+        const NoAllocLayout lay(M, n_items, F, T);
+        CF_REQUIRE(lay.total <= kNoAllocScratchBytes, "cf_evaluate_best_splits_noalloc: level too large for the "
+                                                      "16 MiB fixed scratch");
+        char* base = noalloc_scratch(ctx->device);
+        NodeDesc* d_nodes = reinterpret_cast<NodeDesc*>(base + lay.nodes);
+        EvalItem* d_items = reinterpret_cast<EvalItem*>(base + lay.items);
+        int* d_order = reinterpret_cast<int*>(base + lay.order);
+        int* d_range = reinterpret_cast<int*>(base + lay.range);
+        ItemCandidates* d_cands = reinterpret_cast<ItemCandidates*>(base + lay.cands);
+        int* d_queue = reinterpret_cast<int*>(base + lay.queue);
+        FeatParams* d_packs = reinterpret_cast<FeatParams*>(base + lay.packs);
+        float* d_sorted = reinterpret_cast<float*>(base + lay.sorted);
+        uint16_t* d_ranks = reinterpret_cast<uint16_t*>(base + lay.ranks);
+        cudaStream_t st = ctx->stream;
+        CF_CUDA_CHECK(cudaMemcpyAsync(d_nodes, nodes.data(), sizeof(NodeDesc) * M, cudaMemcpyHostToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(d_items, items.data(), sizeof(EvalItem) * n_items, cudaMemcpyHostToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n_items, cudaMemcpyHostToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(d_range, range.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice, st));
+        // the work queue counter is the only scratch word that must start at zero
+        CF_CUDA_CHECK(cudaMemsetAsync(d_queue, 0, sizeof(int), st));
+        launch(ctx, "prepare_features", dim3((F + 7) / 8), dim3(256), 0, prepare_eval_features_kernel, F, T, features,
+               thresholds, d_packs, d_sorted, d_ranks);
+
+        DsView ds;
+        ds.color = color;
+        ds.depth = reinterpret_cast<const int2*>(depth);
+        ds.n = num_images;
+        ds.width = width;
+        ds.height = height;
+        ds.plane = static_cast<long long>(width) * height;
+        const int budget = std::max(tuning.bins_budget_words, C * (T + 1));
+        const SmemLayout sl(C, T, tuning.ft_max, budget);
+        CF_REQUIRE(sl.total + 4096 <= ctx->smem_per_block_optin,
+                   "split search: classes x thresholds too large for shared memory");
+        EvalArgs args;
+        args.ds = ds;
+        args.samples = reinterpret_cast<const Sample*>(samples);
+        args.nodes = d_nodes;
+        args.node_hist = node_histograms;
+        args.C = C;
+        args.F = F;
+        args.T = T;
+        args.packs = d_packs;
+        args.sorted_thr = d_sorted;
+        args.ranks = d_ranks;
+        args.items = d_items;
+        args.order = d_order;
+        args.n_items = n_items;
+        args.queue = d_queue;
+        args.cands = d_cands;
+        args.ft_max = tuning.ft_max;
+        args.bins_budget = budget;
+        CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(sl.total)));
+        launch(ctx, "level_eval", dim3(std::min(n_items, slots)), dim3(256), sl.total, level_eval_kernel<true>, args);
+        launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F, d_range,
+               d_cands, thresholds, best);
+        CF_CUDA_CHECK(cudaStreamSynchronize(st));
+    });
+}

@@ -146,6 +146,24 @@ cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* 
                                   int num_thresholds, const int8_t* features, const float* thresholds,
                                   cf_split* best);
 
+/* Allocation-free form of cf_evaluate_best_splits. No counterpart in the reference: it exists for
+ * callers that cannot let a library allocate device memory (a host that owns all GPU memory through
+ * its own pool, or a latency-critical loop where cudaMalloc/cudaFree would synchronise the device).
+ * Every input and output is a DEVICE pointer the caller owns: integral images (colour float
+ * [n][3][H][W], depth int32 pairs {sum, valid} [n][H][W]), samples, node histograms uint32 [M][C]
+ * (flip-Both samples counted twice), the feature table int8 [11][F], thresholds float [T][F] and
+ * best [M]; node_offsets [M+1] is a HOST array. Scratch lives in one fixed 16 MiB device array
+ * compiled into the library, so this call allocates nothing; limits: M <= 65536 nodes, at most 65536
+ * work items, F <= 16384, F x T <= 2^20 (larger levels return CF_ERR_INVALID). The first call on a
+ * device looks the array's device address up (make it before any stream capture). Calls share the
+ * array: calls that overlap on the GPU (other threads or streams) race and must be serialised. */
+cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const float* color, const int32_t* depth,
+                                          int num_images, int width, int height, int num_nodes,
+                                          const int64_t* node_offsets, const cf_sample* samples,
+                                          const uint32_t* node_histograms, int num_classes, int num_features,
+                                          int num_thresholds, const int8_t* features, const float* thresholds,
+                                          cf_split* best);
+
 /* ---------------------------------------------------------------------------------------------
  * Tree training
  * ------------------------------------------------------------------------------------------- */
