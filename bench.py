@@ -363,6 +363,7 @@ def main():
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks.summary(),
                 "predict": predict,
+                "levels_tree0": [[n, s, round(ms, 3)] for n, s, ms in trees[0].level_stats()],
                 "feature_evals_per_step": total_evals / args.steps}
         print(json.dumps(line), flush=True)
     ds.close()

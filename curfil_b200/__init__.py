@@ -263,6 +263,21 @@ def evaluate_best_splits(ds, node_offsets, samples, num_classes, features, thres
     return out
 
 
+def level_left_counts(ds, node_offsets, samples, num_classes, features, thresholds):
+    """(best splits, left counts uint32 [M][F][T][C]) as accumulated by the level-batched kernel."""
+    node_offsets = np.ascontiguousarray(node_offsets, np.int64)
+    samples = np.ascontiguousarray(samples, SAMPLE_DTYPE)
+    features = np.ascontiguousarray(features, np.int8)
+    thresholds = np.ascontiguousarray(thresholds, np.float32)
+    T, F = thresholds.shape
+    M = len(node_offsets) - 1
+    best = np.empty(M, SPLIT_DTYPE)
+    left = np.empty((M, F, T, num_classes), np.uint32)
+    _check(lib().cf_level_left_counts(ds.handle, M, _p(node_offsets), _p(samples), int(num_classes), F, T,
+                                      _p(features), _p(thresholds), _p(best), _p(left)))
+    return best, left
+
+
 def evaluate_best_splits_noalloc(ctx, color_ptr, depth_ptr, num_images, width, height, node_offsets, samples_ptr,
                                  node_hist_ptr, num_classes, num_features, num_thresholds, features_ptr,
                                  thresholds_ptr, best_ptr):
@@ -305,6 +320,16 @@ class Tree:
     def set_prior(self, prior):
         prior = np.ascontiguousarray(prior, np.uint32)
         _check(lib().cf_tree_set_prior(self.handle, _p(prior), len(prior)))
+
+    def level_stats(self):
+        """[(open nodes, samples, split-search ms)] per level of the last training."""
+        n = _i32()
+        _check(lib().cf_tree_level_stats(self.handle, 0, ctypes.byref(n), _vp(0), _vp(0), _vp(0)))
+        nodes = np.zeros(n.value, np.int32)
+        samples = np.zeros(n.value, np.int64)
+        ms = np.zeros(n.value, np.float32)
+        _check(lib().cf_tree_level_stats(self.handle, n.value, ctypes.byref(n), _p(nodes), _p(samples), _p(ms)))
+        return list(zip(nodes.tolist(), samples.tolist(), ms.tolist()))
 
     def train_stats(self):
         ev, ms, lv = ctypes.c_int64(), ctypes.c_double(), _i32()

@@ -137,7 +137,7 @@ __device__ __forceinline__ double normalize_score(double s) {
 }
 
 // Classification entropy H_c of a node (score.h:174-189), classes in ascending label order.
-__device__ inline double classification_entropy(int num_present, const uint32_t* present_counts, double total) {
+static __device__ __noinline__ double classification_entropy(int num_present, const uint32_t* present_counts, double total) {
     double hc = 0;
     for (int i = 0; i < num_present; i++) hc = __dadd_rn(hc, entropy_of(static_cast<double>(present_counts[i])));
     hc = __dsub_rn(hc, entropy_of(total));

@@ -1,0 +1,178 @@
+// Threshold bin of one feature response, computed with fast paths that fall back to the exact
+// reference arithmetic whenever the fast result could differ. The bin (number of thresholds the
+// response exceeds) is therefore always identical to the one obtained from the exact double
+// response of random_tree_image.h:564-623.
+//
+// 1. Depth-scaled offsets: the reference computes trunc(RN(v / d)) for integer v and float d > 0.
+//    q = RN(|v| * RN(1/d)) is within 2^-23 relative of |v|/d. If q is farther than 2^-20 q from both
+//    neighbouring integers, floor(q) = floor(|v|/d) and RN(|v|/d) cannot round onto the next integer,
+//    so trunc(RN(v/d)) = sign(v) * floor(q). Otherwise the correctly rounded division is evaluated.
+// 2. Depth features: a = RN(RN(sum/1000)/n) per box. The float estimate fdividef(sum, n) * 0.001f
+//    is within 7 * 2^-24 relative of a (int->float 2^-24, fdividef 2 ulp, constant and product
+//    2^-24 each), so r' = a' - b' is within 4.8e-7 (|a| + |b|) of the exact response r. With
+//    delta = 2e-6 (|a'| + |b'|): if no threshold lies in [r' - delta, r' + delta], every threshold
+//    compares the same against r and r', and the bin is #{t < r' - delta}. Otherwise the two
+//    double divisions of the reference are evaluated and the exact response is binned.
+// 3. Colour features are evaluated exactly (integer-valued float corners summed in double).
+// NaN responses (box outside the image, no valid depth in a box, invalid pixel depth) depend only
+// on integer tests and land in bin T (right of every threshold, `!(r <= t)`).
+#pragma once
+
+#include "device_math.cuh"
+
+namespace cf {
+
+struct EvalPixel {
+    const float* color;   // colour integral of the sample's image, [3][H][W]
+    const int2* depth;    // depth integral of the sample's image, [H][W]
+    int x, y;
+    float d, inv_d;       // depth in metres and RN(1/d); d <= 0 marks an invalid pixel depth
+};
+
+__device__ __forceinline__ EvalPixel make_eval_pixel(const DsView& ds, const Sample& s) {
+    EvalPixel p;
+    p.color = ds.color + static_cast<long long>(s.image) * 3 * ds.plane;
+    p.depth = ds.depth + static_cast<long long>(s.image) * ds.plane;
+    p.x = s.x;
+    p.y = s.y;
+    p.d = s.depth;
+    p.inv_d = s.depth > 0.0f ? __frcp_rn(s.depth) : 0.0f;
+    return p;
+}
+
+// Slow paths, kept out of line so their registers do not weigh on the hot loop.
+static __device__ __noinline__ int exact_norm_abs(float av, float d) { return __float2int_rz(__fdiv_rn(av, d)); }
+
+// trunc(RN(v / d)) of XY::normalize; av = |v| as float
+__device__ __forceinline__ int fast_norm(int v, float av, float d, float inv_d) {
+    if (v == 0) return 0;
+    const float q = __fmul_rn(av, inv_d);   // 0 < q < 2^22 (|v| <= 128, d >= 0.001)
+    // floor(q) on the FMA pipe: adding 1.5 * 2^23 rounds q to the nearest integer
+    const float t = __fadd_rn(q, 12582912.0f);
+    float n = __fsub_rn(t, 12582912.0f);
+    int ni = __float_as_int(t) - 0x4B400000;
+    if (n > q) {
+        n = __fsub_rn(n, 1.0f);
+        ni -= 1;
+    }
+    const float fr = __fsub_rn(q, n);
+    const float margin = __fmul_rn(q, 9.5367431640625e-07f);  // 2^-20
+    const int r = (fr > margin && __fsub_rn(1.0f, fr) > margin) ? ni : exact_norm_abs(av, d);
+    return v < 0 ? -r : r;
+}
+
+// trunc(RN(v / d)) for an int parameter (used outside the hot loop)
+__device__ __forceinline__ int fast_norm(int v, float d, float inv_d) {
+    return fast_norm(v, static_cast<float>(v < 0 ? -v : v), d, inv_d);
+}
+
+// A candidate feature prepared for the hot loop: the eight parameters and their magnitudes as
+// floats (no int->float conversion per evaluation).
+struct __align__(16) EvalFeat {
+    float av[8];          // |o1x|, |o1y|, |o2x|, |o2y|, |r1x|, |r1y|, |r2x|, |r2y|
+    int8_t v[8];          // o1x, o1y, o2x, o2y, r1x, r1y, r2x, r2y
+    uint8_t type, ch1, ch2, pad;
+    uint32_t pad2[3];
+};
+
+__device__ __forceinline__ EvalFeat make_eval_feat(const FeatParams& f) {
+    EvalFeat e;
+    const int8_t v[8] = {f.o1x, f.o1y, f.o2x, f.o2y, f.r1x, f.r1y, f.r2x, f.r2y};
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        e.v[i] = v[i];
+        e.av[i] = static_cast<float>(v[i] < 0 ? -v[i] : v[i]);
+    }
+    e.type = f.type;
+    e.ch1 = f.ch1;
+    e.ch2 = f.ch2;
+    e.pad = 0;
+    e.pad2[0] = e.pad2[1] = e.pad2[2] = 0;
+    return e;
+}
+
+// #{i : sorted[i] < v}
+__device__ __forceinline__ int count_below(const float* sorted, int T, float v) {
+    int lo = 0, n = T;
+    while (n > 0) {
+        const int half = n >> 1;
+        if (sorted[lo + half] < v) {
+            lo += half + 1;
+            n -= half + 1;
+        } else {
+            n = half;
+        }
+    }
+    return lo;
+}
+
+// bin of an exact double response: #{t : !(r <= t)}; r <= t (float t) iff RU(r) <= t
+__device__ __forceinline__ int exact_bin(double r, const float* sorted, int T) {
+    if (isnan(r)) return T;
+    return count_below(sorted, T, __double2float_ru(r));
+}
+
+// exact depth response ((s1/1000)/n1 - (s2/1000)/n2 in double, random_tree_image.h:313-315) binned
+static __device__ __noinline__ int exact_depth_bin(int s1, int nv1, int s2, int nv2, const float* sorted, int T) {
+    const double A = __ddiv_rn(__ddiv_rn(static_cast<double>(s1), 1000.0), static_cast<double>(nv1));
+    const double B = __ddiv_rn(__ddiv_rn(static_cast<double>(s2), 1000.0), static_cast<double>(nv2));
+    return exact_bin(__dsub_rn(A, B), sorted, T);
+}
+
+__device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, const EvalFeat& f, bool flip,
+                                           const float* sorted, int T) {
+    if (!(p.d > 0.0f)) return T;
+    const int o1x = flip ? -f.v[0] : f.v[0];
+    const int o2x = flip ? -f.v[2] : f.v[2];
+    const int x1 = p.x + fast_norm(o1x, f.av[0], p.d, p.inv_d);
+    const int y1 = p.y + fast_norm(f.v[1], f.av[1], p.d, p.inv_d);
+    const int w1 = max(1, fast_norm(f.v[4], f.av[4], p.d, p.inv_d));
+    const int h1 = max(1, fast_norm(f.v[5], f.av[5], p.d, p.inv_d));
+    if (x1 - w1 < 0 || x1 + w1 >= W || y1 - h1 < 0 || y1 + h1 >= H) return T;
+    const int x2 = p.x + fast_norm(o2x, f.av[2], p.d, p.inv_d);
+    const int y2 = p.y + fast_norm(f.v[3], f.av[3], p.d, p.inv_d);
+    const int w2 = max(1, fast_norm(f.v[6], f.av[6], p.d, p.inv_d));
+    const int h2 = max(1, fast_norm(f.v[7], f.av[7], p.d, p.inv_d));
+    if (x2 - w2 < 0 || x2 + w2 >= W || y2 - h2 < 0 || y2 + h2 >= H) return T;
+    const int ul1 = (y1 - h1) * W + (x1 - w1), ur1 = (y1 - h1) * W + (x1 + w1);
+    const int ll1 = (y1 + h1) * W + (x1 - w1), lr1 = (y1 + h1) * W + (x1 + w1);
+    const int ul2 = (y2 - h2) * W + (x2 - w2), ur2 = (y2 - h2) * W + (x2 + w2);
+    const int ll2 = (y2 + h2) * W + (x2 - w2), lr2 = (y2 + h2) * W + (x2 + w2);
+    if (f.type == kDepthFeature) {
+        const int2 a_ul = __ldg(p.depth + ul1), a_ur = __ldg(p.depth + ur1);
+        const int2 a_ll = __ldg(p.depth + ll1), a_lr = __ldg(p.depth + lr1);
+        const int2 b_ul = __ldg(p.depth + ul2), b_ur = __ldg(p.depth + ur2);
+        const int2 b_ll = __ldg(p.depth + ll2), b_lr = __ldg(p.depth + lr2);
+        const int nv1 = (a_lr.y - a_ur.y) + (a_ul.y - a_ll.y);
+        const int nv2 = (b_lr.y - b_ur.y) + (b_ul.y - b_ll.y);
+        if (nv1 == 0 || nv2 == 0) return T;
+        const int s1 = static_cast<int>((static_cast<uint32_t>(a_lr.x) - static_cast<uint32_t>(a_ur.x)) +
+                                        (static_cast<uint32_t>(a_ul.x) - static_cast<uint32_t>(a_ll.x)));
+        const int s2 = static_cast<int>((static_cast<uint32_t>(b_lr.x) - static_cast<uint32_t>(b_ur.x)) +
+                                        (static_cast<uint32_t>(b_ul.x) - static_cast<uint32_t>(b_ll.x)));
+        // 1 <= nv < 2^23 converts exactly through the float bit pattern (no conversion unit)
+        const float n1f = __fsub_rn(__int_as_float(0x4B000000 + nv1), 8388608.0f);
+        const float n2f = __fsub_rn(__int_as_float(0x4B000000 + nv2), 8388608.0f);
+        const float a = __fdividef(static_cast<float>(s1), n1f) * 0.001f;
+        const float b = __fdividef(static_cast<float>(s2), n2f) * 0.001f;
+        const float r = a - b;
+        const float delta = 2e-6f * (fabsf(a) + fabsf(b)) + 1e-30f;
+        const int k = count_below(sorted, T, r - delta);
+        if (k == T || sorted[k] > r + delta) return k;
+        return exact_depth_bin(s1, nv1, s2, nv2, sorted, T);
+    }
+    const float* P1 = p.color + static_cast<long long>(f.ch1) * W * H;
+    const float* P2 = p.color + static_cast<long long>(f.ch2) * W * H;
+    const float c_lr = __ldg(P1 + lr1), c_ur = __ldg(P1 + ur1), c_ul = __ldg(P1 + ul1), c_ll = __ldg(P1 + ll1);
+    const float d_lr = __ldg(P2 + lr2), d_ur = __ldg(P2 + ur2), d_ul = __ldg(P2 + ul2), d_ll = __ldg(P2 + ll2);
+    if (isnan(c_lr) || isnan(c_ur) || isnan(c_ul) || isnan(c_ll) || isnan(d_lr) || isnan(d_ur) || isnan(d_ul) ||
+        isnan(d_ll))
+        return T;
+    const double A = __dadd_rn(__dsub_rn(static_cast<double>(c_lr), static_cast<double>(c_ur)),
+                               __dsub_rn(static_cast<double>(c_ul), static_cast<double>(c_ll)));
+    const double B = __dadd_rn(__dsub_rn(static_cast<double>(d_lr), static_cast<double>(d_ur)),
+                               __dsub_rn(static_cast<double>(d_ul), static_cast<double>(d_ll)));
+    return exact_bin(__dsub_rn(A, B), sorted, T);
+}
+
+}  // namespace cf

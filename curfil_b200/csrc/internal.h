@@ -201,4 +201,10 @@ struct cf_dataset {
     cf::DevArray<int2> depth;    // [n][H][W] integral {depth mm sum (wrapping int32), valid count}
     cf::DevArray<uint8_t> raw_rgb;      // upload staging
     cf::DevArray<uint16_t> raw_depth;
+    // tree-training buffers reused across cf_train_tree calls on this dataset (grow-only)
+    void* trainer = nullptr;
+    void (*trainer_free)(void*) = nullptr;
+    ~cf_dataset() {
+        if (trainer && trainer_free) trainer_free(trainer);
+    }
 };

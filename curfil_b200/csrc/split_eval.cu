@@ -21,6 +21,7 @@
 #include <cstring>
 #include <limits>
 
+#include "eval_fast.cuh"
 #include "split_eval.h"
 
 namespace cf {
@@ -72,6 +73,7 @@ struct EvalArgs {
     ItemCandidates* cands;
     int ft_max;
     int bins_budget;
+    uint32_t* dump_left;   // optional [M][F][T][C] left counts (tests); nullptr in training
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -83,7 +85,7 @@ struct SmemLayout {
         counts = o;
         o += align16(sizeof(uint32_t) * C);
         params = o;
-        o += align16(sizeof(FeatParams) * ft_max);
+        o += align16(sizeof(EvalFeat) * ft_max);
         thr = o;
         o += align16(sizeof(float) * ft_max * T);
         rank = o;
@@ -98,7 +100,7 @@ struct SmemLayout {
 
 // Normalised information gain of one (feature, threshold) from cumulative bins.
 // cum points at bins[f][0][rank]; stride between classes is T + 1.
-__device__ inline double score_from_cum(const uint32_t* cum, int stride, const uint32_t* counts, int cp, double total,
+__device__ __noinline__ double score_from_cum(const uint32_t* cum, int stride, const uint32_t* counts, int cp, double total,
                                         double hc) {
     uint32_t L = 0;
     for (int i = 0; i < cp; i++) L += cum[i * stride];
@@ -123,11 +125,12 @@ __device__ inline double score_from_cum(const uint32_t* cum, int stride, const u
 }
 
 template <bool kAgg>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 level_eval_kernel(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
     __shared__ uint8_t s_lid[256];
+    __shared__ uint8_t s_pc[256];   // dense class id -> label
     __shared__ int s_warp_cnt[8];
     __shared__ int s_cp;
     __shared__ double s_total, s_hc;
@@ -138,7 +141,7 @@ level_eval_kernel(EvalArgs a) {
 
     const SmemLayout L(a.C, a.T, a.ft_max, a.bins_budget);
     uint32_t* s_counts = reinterpret_cast<uint32_t*>(smem + L.counts);
-    FeatParams* s_params = reinterpret_cast<FeatParams*>(smem + L.params);
+    EvalFeat* s_params = reinterpret_cast<EvalFeat*>(smem + L.params);
     float* s_thr = reinterpret_cast<float*>(smem + L.thr);
     uint16_t* s_rank = reinterpret_cast<uint16_t*>(smem + L.rank);
     double* s_scores = reinterpret_cast<double*>(smem + L.scores);
@@ -172,6 +175,7 @@ level_eval_kernel(EvalArgs a) {
             for (int w = 0; w < warp; w++) base += s_warp_cnt[w];
             const int idx = base + __popc(bal & ((1u << lane) - 1u));
             if (tid < 256) s_lid[tid] = present ? static_cast<uint8_t>(idx) : static_cast<uint8_t>(255);
+            if (present) s_pc[idx] = static_cast<uint8_t>(tid);
             if (present) s_counts[idx] = cnt;
             if (tid == 0) {
                 int cp = 0;
@@ -201,7 +205,7 @@ level_eval_kernel(EvalArgs a) {
         for (int f0 = item.f_begin; f0 < item.f_end; f0 += ft) {
             const int nf = min(ft, item.f_end - f0);
             // ---- stage the tile
-            for (int i = tid; i < nf; i += blockDim.x) s_params[i] = a.packs[f0 + i];
+            for (int i = tid; i < nf; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[f0 + i]);
             for (int i = tid; i < nf * T; i += blockDim.x) {
                 s_thr[i] = a.sorted_thr[static_cast<long long>(f0) * T + i];
                 s_rank[i] = a.ranks[static_cast<long long>(f0) * T + i];
@@ -210,35 +214,84 @@ level_eval_kernel(EvalArgs a) {
             for (int i = tid; i < nbins; i += blockDim.x) s_bins[i] = 0u;
             __syncthreads();
 
-            // ---- histogram: pairs p = f * N + s, uniform trip count so warps stay converged
-            const long long pairs = static_cast<long long>(nf) * N;
-            const int iters = static_cast<int>((pairs + blockDim.x - 1) / blockDim.x);
-            const int stride = blockDim.x;
-            const int qstep = stride / N;
-            const int rstep = stride - qstep * N;
-            int f = tid / N;
-            int s = tid - f * N;
-            for (int it = 0; it < iters; it++) {
-                int key1 = -1, key2 = -1;
-                if (f < nf) {
-                    const Sample smp = a.samples[nd.start + s];
-                    const FeatParams fp = s_params[f];
-                    const float* sorted = s_thr + f * T;
-                    const int row = (f * cp + s_lid[smp.label]) * T1;
-                    if (smp.flip == 2) {
-                        key1 = row + bin_of(sample_response(a.ds, smp, fp, false), sorted, T);
-                        key2 = row + bin_of(sample_response(a.ds, smp, fp, true), sorted, T);
-                    } else {
-                        key1 = row + bin_of(sample_response(a.ds, smp, fp, smp.flip == 1), sorted, T);
+            const int W = a.ds.width, H = a.ds.height;
+            if (N >= static_cast<int>(blockDim.x)) {
+                // ---- histogram, sample-major: each thread keeps one sample and walks the tile's
+                // features, so the sample's neighbourhood is reused from L1 across features
+                for (int s0 = 0; s0 < N; s0 += blockDim.x) {
+                    const int s = s0 + tid;
+                    const bool valid = s < N;
+                    EvalPixel px;
+                    int lid = 0, flip = 0;
+                    if (valid) {
+                        const Sample smp = a.samples[nd.start + s];
+                        px = make_eval_pixel(a.ds, smp);
+                        lid = s_lid[smp.label];
+                        flip = smp.flip;
+                    }
+                    const bool any_both = __any_sync(kFull, flip == 2);
+                    // two features per step: their evaluations are independent, so their gathers and
+                    // arithmetic overlap before the two warp-synchronous increments
+                    int f = 0;
+                    for (; f + 1 < nf; f += 2) {
+                        const EvalFeat& fa = s_params[f];
+                        const EvalFeat& fb = s_params[f + 1];
+                        const int row_a = (f * cp + lid) * T1;
+                        const int row_b = ((f + 1) * cp + lid) * T1;
+                        const int ka = valid ? row_a + feature_bin(px, W, H, fa, flip == 1, s_thr + f * T, T) : -1;
+                        const int kb =
+                            valid ? row_b + feature_bin(px, W, H, fb, flip == 1, s_thr + (f + 1) * T, T) : -1;
+                        bin_increment<kAgg>(s_bins, ka);
+                        bin_increment<kAgg>(s_bins, kb);
+                        if (any_both) {
+                            const int ka2 = flip == 2 ? row_a + feature_bin(px, W, H, fa, true, s_thr + f * T, T) : -1;
+                            const int kb2 =
+                                flip == 2 ? row_b + feature_bin(px, W, H, fb, true, s_thr + (f + 1) * T, T) : -1;
+                            bin_increment<kAgg>(s_bins, ka2);
+                            bin_increment<kAgg>(s_bins, kb2);
+                        }
+                    }
+                    if (f < nf) {
+                        const EvalFeat& fp = s_params[f];
+                        const float* sorted = s_thr + f * T;
+                        const int row = (f * cp + lid) * T1;
+                        const int key1 = valid ? row + feature_bin(px, W, H, fp, flip == 1, sorted, T) : -1;
+                        bin_increment<kAgg>(s_bins, key1);
+                        if (any_both) {
+                            const int key2 = flip == 2 ? row + feature_bin(px, W, H, fp, true, sorted, T) : -1;
+                            bin_increment<kAgg>(s_bins, key2);
+                        }
                     }
                 }
-                bin_increment<kAgg>(s_bins, key1);
-                if (__any_sync(kFull, key2 >= 0)) bin_increment<kAgg>(s_bins, key2);
-                s += rstep;
-                f += qstep;
-                if (s >= N) {
-                    s -= N;
-                    f++;
+            } else {
+                // ---- histogram, pair-major for small nodes: pairs p = f * N + s, uniform trip count
+                // so warps stay converged
+                const long long pairs = static_cast<long long>(nf) * N;
+                const int iters = static_cast<int>((pairs + blockDim.x - 1) / blockDim.x);
+                const int stride = blockDim.x;
+                const int qstep = stride / N;
+                const int rstep = stride - qstep * N;
+                int f = tid / N;
+                int s = tid - f * N;
+                for (int it = 0; it < iters; it++) {
+                    int key1 = -1, key2 = -1;
+                    if (f < nf) {
+                        const Sample smp = a.samples[nd.start + s];
+                        const EvalPixel px = make_eval_pixel(a.ds, smp);
+                        const EvalFeat& fp = s_params[f];
+                        const float* sorted = s_thr + f * T;
+                        const int row = (f * cp + s_lid[smp.label]) * T1;
+                        key1 = row + feature_bin(px, W, H, fp, smp.flip == 1, sorted, T);
+                        if (smp.flip == 2) key2 = row + feature_bin(px, W, H, fp, true, sorted, T);
+                    }
+                    bin_increment<kAgg>(s_bins, key1);
+                    if (__any_sync(kFull, key2 >= 0)) bin_increment<kAgg>(s_bins, key2);
+                    s += rstep;
+                    f += qstep;
+                    if (s >= N) {
+                        s -= N;
+                        f++;
+                    }
                 }
             }
             __syncthreads();
@@ -253,6 +306,19 @@ level_eval_kernel(EvalArgs a) {
                 }
             }
             __syncthreads();
+
+            if (a.dump_left) {
+                // test hook: left counts of every (feature, threshold, class) of the tile
+                const int n = nf * T * cp;
+                for (int i = tid; i < n; i += blockDim.x) {
+                    const int fl = i / (T * cp);
+                    const int rem = i - fl * T * cp;
+                    const int t = rem / cp;
+                    const int lid = rem - t * cp;
+                    const uint32_t v = s_bins[(fl * cp + lid) * T1 + s_rank[fl * T + t]];
+                    a.dump_left[((static_cast<long long>(item.node) * a.F + f0 + fl) * T + t) * a.C + s_pc[lid]] = v;
+                }
+            }
 
             // ---- scores of every (feature, threshold) of the tile
             for (int i = tid; i < nf * T; i += blockDim.x) {
@@ -469,7 +535,7 @@ __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const 
 // ------------------------------------------------------------------------------------------------
 void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
                               const uint32_t* node_hist_dev, int M, const std::vector<int>& node_counts, int C,
-                              const LevelFeatures& lf, cf_split* splits_dev) {
+                              const LevelFeatures& lf, cf_split* splits_dev, uint32_t* dump_left) {
     const int F = lf.F, T = lf.T;
     CF_REQUIRE(C >= 1 && C <= 256, "number of classes must be in [1, 256]");
     CF_REQUIRE(T >= 1 && T <= 4096, "number of thresholds must be in [1, 4096]");
@@ -542,6 +608,7 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     args.cands = cands_.get();
     args.ft_max = tuning.ft_max;
     args.bins_budget = budget;
+    args.dump_left = dump_left;
     const int grid = std::min(n_items, slots);
     if (tuning.warp_aggregate) {
         CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -820,6 +887,7 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         args.cands = d_cands;
         args.ft_max = tuning.ft_max;
         args.bins_budget = budget;
+        args.dump_left = nullptr;
         CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(sl.total)));
         launch(ctx, "level_eval", dim3(std::min(n_items, slots)), dim3(256), sl.total, level_eval_kernel<true>, args);

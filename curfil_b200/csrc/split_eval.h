@@ -48,7 +48,7 @@ public:
     // node_counts: the M sample counts on the host (for work-item sizing).
     void evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
                   const uint32_t* node_hist_dev, int M, const std::vector<int>& node_counts, int C,
-                  const LevelFeatures& lf, cf_split* splits_dev);
+                  const LevelFeatures& lf, cf_split* splits_dev, uint32_t* dump_left = nullptr);
     EvalTuning tuning;
     int64_t last_items = 0;
 

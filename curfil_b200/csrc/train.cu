@@ -48,6 +48,11 @@ void validate_thresholds(const float* thr, long long n) {
 class TreeTrainer {
 public:
     TreeTrainer(cf_dataset* ds, int C, const cf_train_config& cfg, int mode) : ds_(ds), C_(C), cfg_(cfg), mode_(mode) {}
+    void configure(int C, const cf_train_config& cfg, int mode) {
+        C_ = C;
+        cfg_ = cfg;
+        mode_ = mode;
+    }
 
     cf_tree* train(const cf_sample* host_samples, int N, int tree_id, int32_t* seed_counter) {
         cf_context* ctx = ds_->ctx;
@@ -112,6 +117,9 @@ public:
         int tree_next = 1;
         int64_t evals = 0;
         int levels = 0;
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> level_events;
+        std::vector<int32_t> level_nodes;
+        std::vector<int64_t> level_samples;
         std::vector<NodeDesc> h_nodes;
         std::vector<int> counts;
         while (M > 0 && level < cfg_.max_depth) {
@@ -125,6 +133,13 @@ public:
             CF_CUDA_CHECK(cudaStreamSynchronize(st));
             counts.resize(M);
             for (int i = 0; i < M; i++) counts[i] = h_nodes[i].count;
+            cudaEvent_t le0, le1;
+            CF_CUDA_CHECK(cudaEventCreate(&le0));
+            CF_CUDA_CHECK(cudaEventCreate(&le1));
+            CF_CUDA_CHECK(cudaEventRecord(le0, st));
+            level_events.emplace_back(le0, le1);
+            level_nodes.push_back(M);
+            level_samples.push_back(n);
             if (mode_ == CF_TRAIN_PER_NODE) {
                 for (int i = 0; i < M; i++)
                     plain_.evaluate_node(ctx, ds, samples_[cur].get(), h_nodes[i].start, h_nodes[i].count,
@@ -134,6 +149,7 @@ public:
                 eval_.evaluate(ctx, ds, samples_[cur].get(), nodes_[cur].get(), hist_[cur].get(), M, counts, C_, lf_,
                                splits_.get());
             }
+            CF_CUDA_CHECK(cudaEventRecord(le1, st));
             evals += n * F;
             levels++;
             const bool scatter = level + 1 < cfg_.max_depth;
@@ -181,6 +197,15 @@ public:
         t->feature_evals = evals;
         t->device_ms = ms;
         t->levels = levels;
+        t->level_nodes = level_nodes;
+        t->level_samples = level_samples;
+        for (auto& pr : level_events) {
+            float lms = 0;
+            cudaEventElapsedTime(&lms, pr.first, pr.second);
+            t->level_eval_ms.push_back(lms);
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
         return t;
     }
 
@@ -206,8 +231,14 @@ private:
 
 cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
                     int32_t* seed_counter, int mode) {
-    TreeTrainer trainer(ds, C, cfg, mode);
-    return trainer.train(samples, N, tree_id, seed_counter);
+    // the dataset keeps one trainer so its device buffers are allocated once, not per tree
+    if (ds->trainer == nullptr) {
+        ds->trainer = new TreeTrainer(ds, C, cfg, mode);
+        ds->trainer_free = [](void* p) { delete static_cast<TreeTrainer*>(p); };
+    }
+    TreeTrainer* trainer = static_cast<TreeTrainer*>(ds->trainer);
+    trainer->configure(C, cfg, mode);
+    return trainer->train(samples, N, tree_id, seed_counter);
 }
 
 }  // namespace cf
@@ -331,10 +362,16 @@ cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample*
     });
 }
 
-cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* node_offsets, const cf_sample* samples,
-                                  int num_classes, int num_features, int num_thresholds, const int8_t* features,
-                                  const float* thresholds, cf_split* best) {
-    return guard([&] {
+}  // extern "C"
+
+namespace {
+
+// evaluateBestSplits on host buffers; with `left_counts` the kernel also reports its left counts
+// [M][F][T][C] (class = label).
+void evaluate_level_host(cf_dataset* ds, int num_nodes, const int64_t* node_offsets, const cf_sample* samples,
+                         int num_classes, int num_features, int num_thresholds, const int8_t* features,
+                         const float* thresholds, cf_split* best, uint32_t* left_counts) {
+    {
         CF_REQUIRE(ds && node_offsets && samples && features && thresholds && best, "cf_evaluate_best_splits: NULL argument");
         CF_REQUIRE(num_nodes > 0 && num_features > 0 && num_thresholds > 0, "cf_evaluate_best_splits: empty input");
         CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_evaluate_best_splits: classes must be in [1, 256]");
@@ -374,11 +411,43 @@ cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* 
                                       cudaMemcpyHostToDevice, ctx->stream));
         prepare_eval_features(ctx, lf);
         LevelEvaluator ev;
+        DevArray<uint32_t> d_left;
+        const size_t n_left = static_cast<size_t>(num_nodes) * num_features * num_thresholds * num_classes;
+        if (left_counts) {
+            d_left.reserve(n_left);
+            CF_CUDA_CHECK(cudaMemsetAsync(d_left.get(), 0, sizeof(uint32_t) * n_left, ctx->stream));
+        }
         ev.evaluate(ctx, view_of(ds), u.samples.get(), d_nodes.get(), d_hist.get(), num_nodes, counts, num_classes, lf,
-                    d_best.get());
+                    d_best.get(), left_counts ? d_left.get() : nullptr);
         CF_CUDA_CHECK(cudaMemcpyAsync(best, d_best.get(), sizeof(cf_split) * num_nodes, cudaMemcpyDeviceToHost,
                                       ctx->stream));
+        if (left_counts)
+            CF_CUDA_CHECK(cudaMemcpyAsync(left_counts, d_left.get(), sizeof(uint32_t) * n_left, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
         CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* node_offsets, const cf_sample* samples,
+                                  int num_classes, int num_features, int num_thresholds, const int8_t* features,
+                                  const float* thresholds, cf_split* best) {
+    return guard([&] {
+        evaluate_level_host(ds, num_nodes, node_offsets, samples, num_classes, num_features, num_thresholds, features,
+                            thresholds, best, nullptr);
+    });
+}
+
+cf_status cf_level_left_counts(cf_dataset* ds, int num_nodes, const int64_t* node_offsets, const cf_sample* samples,
+                               int num_classes, int num_features, int num_thresholds, const int8_t* features,
+                               const float* thresholds, cf_split* best, uint32_t* left_counts) {
+    return guard([&] {
+        CF_REQUIRE(left_counts, "cf_level_left_counts: left_counts is NULL");
+        evaluate_level_host(ds, num_nodes, node_offsets, samples, num_classes, num_features, num_thresholds, features,
+                            thresholds, best, left_counts);
     });
 }
 
@@ -458,6 +527,21 @@ cf_status cf_tree_import(int tree_id, int num_nodes, int num_classes, const int3
 
 cf_status cf_tree_destroy(cf_tree* tree) {
     return guard([&] { delete tree; });
+}
+
+cf_status cf_tree_level_stats(cf_tree* tree, int capacity, int* num_levels, int32_t* nodes, int64_t* samples,
+                              float* eval_ms) {
+    return guard([&] {
+        CF_REQUIRE(tree && num_levels, "cf_tree_level_stats: NULL argument");
+        const int n = static_cast<int>(tree->level_eval_ms.size());
+        *num_levels = n;
+        const int m = std::min(n, capacity);
+        for (int i = 0; i < m; i++) {
+            if (nodes) nodes[i] = tree->level_nodes[i];
+            if (samples) samples[i] = tree->level_samples[i];
+            if (eval_ms) eval_ms[i] = tree->level_eval_ms[i];
+        }
+    });
 }
 
 cf_status cf_tree_train_stats(cf_tree* tree, int64_t* feature_evals, double* device_ms, int* levels) {

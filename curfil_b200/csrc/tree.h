@@ -20,6 +20,9 @@ struct cf_tree {
     int64_t feature_evals = 0;
     double device_ms = 0.0;
     int levels = 0;
+    std::vector<int32_t> level_nodes;     // open nodes evaluated per level
+    std::vector<int64_t> level_samples;   // samples of those nodes
+    std::vector<float> level_eval_ms;     // device time of the split search per level
 
     void resize(int n) {
         num_nodes = n;

@@ -146,6 +146,14 @@ cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* 
                                   int num_thresholds, const int8_t* features, const float* thresholds,
                                   cf_split* best);
 
+/* cf_evaluate_best_splits that also returns the counts the level-batched kernel accumulated:
+ * left_counts uint32 [M][F][T][C] (samples of node m, class c, with response <= threshold t), the
+ * left half of the counters of calculateFeatureResponsesAndHistograms (random_tree_image_gpu.cu:1958-2135)
+ * for every node of the level. For verification; training never materialises these counts. */
+cf_status cf_level_left_counts(cf_dataset* ds, int num_nodes, const int64_t* node_offsets,
+                               const cf_sample* samples, int num_classes, int num_features,
+                               int num_thresholds, const int8_t* features, const float* thresholds,
+                               cf_split* best, uint32_t* left_counts);
 /* Allocation-free form of cf_evaluate_best_splits. No counterpart in the reference: it exists for
  * callers that cannot let a library allocate device memory (a host that owns all GPU memory through
  * its own pool, or a latency-critical loop where cudaMalloc/cudaFree would synchronise the device).
@@ -212,6 +220,10 @@ cf_status cf_tree_prior(cf_tree* tree, uint32_t* prior, int capacity, int* count
 cf_status cf_tree_set_prior(cf_tree* tree, const uint32_t* prior, int count);
 /* Per-level statistics of the last training of this tree: feature evaluations and device time. */
 cf_status cf_tree_train_stats(cf_tree* tree, int64_t* feature_evals, double* device_ms, int* levels);
+/* Per level of the last training: open nodes, their samples and the device time of the split search
+ * (the reference logs per-level times, random_tree.h:1259,1411). Copies min(capacity, levels) entries. */
+cf_status cf_tree_level_stats(cf_tree* tree, int capacity, int* num_levels, int32_t* nodes, int64_t* samples,
+                              float* eval_ms);
 
 /* ---------------------------------------------------------------------------------------------
  * Prediction: RandomForestImage::normalizeHistograms + convertTree + predict

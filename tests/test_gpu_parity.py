@@ -207,6 +207,28 @@ def test_evaluate_best_splits_level(ctx, scene):
             assert g["threshold"] == th[t, f]
 
 
+@pytest.mark.parametrize("flips", [False, True])
+def test_level_batched_counts_bit_exact(ctx, scene, flips):
+    """The level-batched kernel's accumulated counts equal the oracle's per-node counters exactly
+    (this exercises its fast paths: fallback-checked divisions and float depth estimates)."""
+    rng = np.random.default_rng(33 + flips)
+    sizes = [1500, 1, 7, 300, 64, 2]
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    s = H.random_samples(rng, 4, 96, 72, 40, int(offsets[-1]), depth=scene["depth"], flips=flips)
+    # a few samples with invalid depth and on the image border
+    s["depth"][5] = 0.0
+    s["x"][6], s["y"][6] = 0, 0
+    s["x"][7], s["y"][7] = 95, 71
+    fe, th = orc.generate_features(scene["ods"], s, 99, 96, 12, 60, 15)
+    th[3, :] = th[2, :]               # tied thresholds
+    th[4, :5] = 0.0
+    best, left = cf.level_left_counts(scene["ds"], offsets, s, 40, fe, th)
+    for i in range(len(sizes)):
+        sl = s[offsets[i]:offsets[i + 1]]
+        o = orc.histograms(scene["ods"], sl.view(orc.SAMPLE_DTYPE), fe, th, 40, threads=4)   # [C][F][T][2]
+        np.testing.assert_array_equal(left[i], o[:, :, :, 0].transpose(1, 2, 0), err_msg="node %d" % i)
+
+
 def train_cfg(**kw):
     d = dict(feature_count=120, thresholds=10, max_depth=8, min_sample_count=4, box_radius=40, region_size=10)
     d.update(kw)
