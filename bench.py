@@ -208,6 +208,8 @@ def main():
     ap.add_argument("--trees", type=int, default=W["trees"])
     ap.add_argument("--max-depth", type=int, default=W["max_depth"])
     ap.add_argument("--predict-images", type=int, default=W["predict_images"])
+    ap.add_argument("--tuning", default="", help="split-search launch shape overrides, e.g. ctas_per_sm=4,"
+                    "bins_budget_words=10240 (cf_eval_tuning field names)")
     args = ap.parse_args()
     W.update(images=args.images, trees=args.trees, max_depth=args.max_depth,
              predict_images=min(args.predict_images, args.images))
@@ -249,6 +251,12 @@ def main():
     rgb, depth, labels = make_data()
     cfg = train_config()
     ctx = cf.Context(local)
+    if args.tuning:
+        overrides = {}
+        for kv in args.tuning.split(","):
+            k, v = kv.split("=")
+            overrides[k.strip()] = float(v) if k.strip() == "items_per_slot" else int(v)
+        ctx.set_tuning(**overrides)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
     ds = cf.Dataset.from_raw(ctx, rgb, depth)
@@ -354,7 +362,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "feature-evals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": dict(workload_config(), parallelism="trees sharded over %d GPU(s)" % world),
+                "config": dict(workload_config(), parallelism="trees sharded over %d GPU(s)" % world,
+                               split_search_tuning=ctx.get_tuning().as_dict()),
                 "roofline": {"bound": "hbm", "kernel": "level_eval", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                              "peak_source": peak_kind, "bytes_per_eval": bytes_per_eval,

@@ -61,6 +61,16 @@ class ServerConfig(ctypes.Structure):
                 ("return_probabilities", ctypes.c_int32)]
 
 
+class EvalTuning(ctypes.Structure):
+    """cf_eval_tuning: launch shape of the level-batched split search (speed only, never results)."""
+    _fields_ = [("features_per_tile", ctypes.c_int32), ("bins_budget_words", ctypes.c_int32),
+                ("warp_aggregate", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("feature_granule", ctypes.c_int32), ("items_per_slot", ctypes.c_float)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class RequestStats(ctypes.Structure):
     _fields_ = [("submit_ms", ctypes.c_double), ("admitted_ms", ctypes.c_double), ("done_ms", ctypes.c_double),
                 ("batch_id", ctypes.c_int32), ("batch_frames", ctypes.c_int32)]
@@ -147,6 +157,24 @@ class Context:
 
     def launch_count(self):
         return lib().cf_context_launch_count(self.handle)
+
+    def get_tuning(self):
+        t = EvalTuning()
+        _check(lib().cf_context_get_tuning(self.handle, ctypes.byref(t)))
+        return t
+
+    def set_tuning(self, tuning=None, **fields):
+        """Set the split-search launch shape: an EvalTuning, and/or field=value overrides of the
+        current one; no arguments restore the defaults."""
+        if tuning is None and not fields:
+            _check(lib().cf_context_set_tuning(self.handle, _vp(0)))
+            return
+        t = self.get_tuning() if tuning is None else EvalTuning(*[getattr(tuning, n) for n, _ in EvalTuning._fields_])
+        for k, v in fields.items():
+            if k not in dict(EvalTuning._fields_):
+                raise ValueError("unknown tuning field %r" % k)
+            setattr(t, k, v)
+        _check(lib().cf_context_set_tuning(self.handle, ctypes.byref(t)))
 
 
 class Dataset:

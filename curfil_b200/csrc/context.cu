@@ -183,4 +183,31 @@ cf_status cf_context_reset_timing(cf_context* ctx) {
 
 int64_t cf_context_launch_count(cf_context* ctx) { return ctx ? ctx->launches.load() : 0; }
 
+cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out) {
+    return cf::guard([&] {
+        CF_REQUIRE(ctx && out, "cf_context_get_tuning: NULL argument");
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        *out = ctx->tuning;
+    });
+}
+
+cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning) {
+    return cf::guard([&] {
+        CF_REQUIRE(ctx, "cf_context_set_tuning: ctx is NULL");
+        const cf_eval_tuning t = tuning ? *tuning : cf_context::default_tuning();
+        CF_REQUIRE(t.features_per_tile >= 2 && t.features_per_tile <= 64,
+                   "cf_context_set_tuning: features_per_tile must be in [2, 64]");
+        CF_REQUIRE(t.bins_budget_words >= 1024 && t.bins_budget_words <= 49152,
+                   "cf_context_set_tuning: bins_budget_words must be in [1024, 49152]");
+        CF_REQUIRE(t.warp_aggregate == 0 || t.warp_aggregate == 1, "cf_context_set_tuning: warp_aggregate is 0 or 1");
+        CF_REQUIRE(t.ctas_per_sm >= 1 && t.ctas_per_sm <= 4, "cf_context_set_tuning: ctas_per_sm must be in [1, 4]");
+        CF_REQUIRE(t.feature_granule >= 1 && t.feature_granule <= 64,
+                   "cf_context_set_tuning: feature_granule must be in [1, 64]");
+        CF_REQUIRE(t.items_per_slot > 0.0f && t.items_per_slot <= 1024.0f,
+                   "cf_context_set_tuning: items_per_slot must be in (0, 1024]");
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        ctx->tuning = t;
+    });
+}
+
 }  // extern "C"

@@ -4,9 +4,11 @@
 // response of random_tree_image.h:564-623.
 //
 // 1. Depth-scaled offsets: the reference computes trunc(RN(v / d)) for integer v and float d > 0.
-//    q = RN(|v| * RN(1/d)) is within 2^-23 relative of |v|/d. If q is farther than 2^-20 q from both
-//    neighbouring integers, floor(q) = floor(|v|/d) and RN(|v|/d) cannot round onto the next integer,
-//    so trunc(RN(v/d)) = sign(v) * floor(q). Otherwise the correctly rounded division is evaluated.
+//    q = RN(|v| * RN(1/d)) and y = RN(|v|/d) both lie within q (1 +- 2^-22). lo = RD(q (1 - 2^-21))
+//    and hi = RU(q (1 + 2^-21)) bracket y; when floor(lo) == floor(hi) that is floor(y), so
+//    trunc(RN(v/d)) = sign(v) * floor(lo). Otherwise the correctly rounded division is evaluated.
+//    floor() of a value in [0, 2^23) is taken on the FMA pipe: RD(x + 2^23) = 2^23 + floor(x).
+//    (d >= 0.001 because pixel depths are integer millimetres, so q <= 127000 < 2^23.)
 // 2. Depth features: a = RN(RN(sum/1000)/n) per box. The float estimate fdividef(sum, n) * 0.001f
 //    is within 7 * 2^-24 relative of a (int->float 2^-24, fdividef 2 ulp, constant and product
 //    2^-24 each), so r' = a' - b' is within 4.8e-7 (|a| + |b|) of the exact response r. With
@@ -43,21 +45,15 @@ __device__ __forceinline__ EvalPixel make_eval_pixel(const DsView& ds, const Sam
 // Slow paths, kept out of line so their registers do not weigh on the hot loop.
 static __device__ __noinline__ int exact_norm_abs(float av, float d) { return __float2int_rz(__fdiv_rn(av, d)); }
 
-// trunc(RN(v / d)) of XY::normalize; av = |v| as float
+// trunc(RN(v / d)) of XY::normalize; av = |v| as float (0 gives 0 without a special case)
 __device__ __forceinline__ int fast_norm(int v, float av, float d, float inv_d) {
-    if (v == 0) return 0;
-    const float q = __fmul_rn(av, inv_d);   // 0 < q < 2^22 (|v| <= 128, d >= 0.001)
-    // floor(q) on the FMA pipe: adding 1.5 * 2^23 rounds q to the nearest integer
-    const float t = __fadd_rn(q, 12582912.0f);
-    float n = __fsub_rn(t, 12582912.0f);
-    int ni = __float_as_int(t) - 0x4B400000;
-    if (n > q) {
-        n = __fsub_rn(n, 1.0f);
-        ni -= 1;
-    }
-    const float fr = __fsub_rn(q, n);
-    const float margin = __fmul_rn(q, 9.5367431640625e-07f);  // 2^-20
-    const int r = (fr > margin && __fsub_rn(1.0f, fr) > margin) ? ni : exact_norm_abs(av, d);
+    const float q = __fmul_rn(av, inv_d);
+    const float lo = __fmaf_rd(q, -4.76837158203125e-07f, q);   // q (1 - 2^-21), rounded down
+    const float hi = __fmaf_ru(q, 4.76837158203125e-07f, q);    // q (1 + 2^-21), rounded up
+    const float tl = __fadd_rd(lo, 8388608.0f);                 // 2^23 + floor(lo)
+    const float th = __fadd_rd(hi, 8388608.0f);
+    int r = __float_as_int(tl) - 0x4B000000;
+    if (tl != th) r = exact_norm_abs(av, d);
     return v < 0 ? -r : r;
 }
 
@@ -91,8 +87,21 @@ __device__ __forceinline__ EvalFeat make_eval_feat(const FeatParams& f) {
     return e;
 }
 
+// Thresholds of one feature in shared memory: sorted ascending; with kPad32 (T <= 31) the row has 32
+// entries, positions T..31 holding +inf, and is searched branch-free in five steps.
+constexpr int kPadThresholds = 32;
+
 // #{i : sorted[i] < v}
+template <bool kPad32>
 __device__ __forceinline__ int count_below(const float* sorted, int T, float v) {
+    if (kPad32) {
+        int k = sorted[15] < v ? 16 : 0;
+        k += sorted[k + 7] < v ? 8 : 0;
+        k += sorted[k + 3] < v ? 4 : 0;
+        k += sorted[k + 1] < v ? 2 : 0;
+        k += sorted[k] < v ? 1 : 0;
+        return k;
+    }
     int lo = 0, n = T;
     while (n > 0) {
         const int half = n >> 1;
@@ -107,18 +116,21 @@ __device__ __forceinline__ int count_below(const float* sorted, int T, float v) 
 }
 
 // bin of an exact double response: #{t : !(r <= t)}; r <= t (float t) iff RU(r) <= t
+template <bool kPad32>
 __device__ __forceinline__ int exact_bin(double r, const float* sorted, int T) {
     if (isnan(r)) return T;
-    return count_below(sorted, T, __double2float_ru(r));
+    return count_below<kPad32>(sorted, T, __double2float_ru(r));
 }
 
 // exact depth response ((s1/1000)/n1 - (s2/1000)/n2 in double, random_tree_image.h:313-315) binned
+template <bool kPad32>
 static __device__ __noinline__ int exact_depth_bin(int s1, int nv1, int s2, int nv2, const float* sorted, int T) {
     const double A = __ddiv_rn(__ddiv_rn(static_cast<double>(s1), 1000.0), static_cast<double>(nv1));
     const double B = __ddiv_rn(__ddiv_rn(static_cast<double>(s2), 1000.0), static_cast<double>(nv2));
-    return exact_bin(__dsub_rn(A, B), sorted, T);
+    return exact_bin<kPad32>(__dsub_rn(A, B), sorted, T);
 }
 
+template <bool kPad32>
 __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, const EvalFeat& f, bool flip,
                                            const float* sorted, int T) {
     if (!(p.d > 0.0f)) return T;
@@ -157,9 +169,9 @@ __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, con
         const float b = __fdividef(static_cast<float>(s2), n2f) * 0.001f;
         const float r = a - b;
         const float delta = 2e-6f * (fabsf(a) + fabsf(b)) + 1e-30f;
-        const int k = count_below(sorted, T, r - delta);
-        if (k == T || sorted[k] > r + delta) return k;
-        return exact_depth_bin(s1, nv1, s2, nv2, sorted, T);
+        const int k = count_below<kPad32>(sorted, T, r - delta);
+        if ((!kPad32 && k == T) || sorted[k] > r + delta) return k;
+        return exact_depth_bin<kPad32>(s1, nv1, s2, nv2, sorted, T);
     }
     const float* P1 = p.color + static_cast<long long>(f.ch1) * W * H;
     const float* P2 = p.color + static_cast<long long>(f.ch2) * W * H;
@@ -172,7 +184,7 @@ __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, con
                                __dsub_rn(static_cast<double>(c_ul), static_cast<double>(c_ll)));
     const double B = __dadd_rn(__dsub_rn(static_cast<double>(d_lr), static_cast<double>(d_ur)),
                                __dsub_rn(static_cast<double>(d_ul), static_cast<double>(d_ll)));
-    return exact_bin(__dsub_rn(A, B), sorted, T);
+    return exact_bin<kPad32>(__dsub_rn(A, B), sorted, T);
 }
 
 }  // namespace cf

@@ -78,16 +78,17 @@ struct EvalArgs {
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// TP = stride of a feature's threshold row (T, or 32 for the padded search)
 struct SmemLayout {
     size_t counts, params, thr, rank, scores, bins, total;
-    __host__ __device__ SmemLayout(int C, int T, int ft_max, int budget) {
+    __host__ __device__ SmemLayout(int C, int T, int TP, int ft_max, int budget) {
         size_t o = 0;
         counts = o;
         o += align16(sizeof(uint32_t) * C);
         params = o;
         o += align16(sizeof(EvalFeat) * ft_max);
         thr = o;
-        o += align16(sizeof(float) * ft_max * T);
+        o += align16(sizeof(float) * ft_max * TP);
         rank = o;
         o += align16(sizeof(uint16_t) * ft_max * T);
         scores = o;
@@ -124,8 +125,8 @@ __device__ __noinline__ double score_from_cum(const uint32_t* cum, int stride, c
     return normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, hc)));
 }
 
-template <bool kAgg>
-__global__ void __launch_bounds__(256, 3)
+template <bool kAgg, bool kPad32, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks)
 level_eval_kernel(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
@@ -137,9 +138,11 @@ level_eval_kernel(EvalArgs a) {
     __shared__ double s_best;
     __shared__ double s_cs[kMaxCand];
     __shared__ int s_ct[kMaxCand], s_cf[kMaxCand];
-    __shared__ int s_cn, s_ovf;
+    __shared__ int s_cn;
+    __shared__ double s_drop;
 
-    const SmemLayout L(a.C, a.T, a.ft_max, a.bins_budget);
+    const int TP = kPad32 ? kPadThresholds : a.T;
+    const SmemLayout L(a.C, a.T, TP, a.ft_max, a.bins_budget);
     uint32_t* s_counts = reinterpret_cast<uint32_t*>(smem + L.counts);
     EvalFeat* s_params = reinterpret_cast<EvalFeat*>(smem + L.params);
     float* s_thr = reinterpret_cast<float*>(smem + L.thr);
@@ -183,7 +186,7 @@ level_eval_kernel(EvalArgs a) {
                 s_cp = cp;
                 s_best = -INFINITY;
                 s_cn = 0;
-                s_ovf = 0;
+                s_drop = -INFINITY;
             }
             __syncthreads();
             if (tid == 0) {
@@ -206,90 +209,92 @@ level_eval_kernel(EvalArgs a) {
             const int nf = min(ft, item.f_end - f0);
             // ---- stage the tile
             for (int i = tid; i < nf; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[f0 + i]);
-            for (int i = tid; i < nf * T; i += blockDim.x) {
-                s_thr[i] = a.sorted_thr[static_cast<long long>(f0) * T + i];
-                s_rank[i] = a.ranks[static_cast<long long>(f0) * T + i];
+            const float* g_thr = a.sorted_thr + static_cast<long long>(f0) * T;
+            if (kPad32) {
+                for (int i = tid; i < nf * kPadThresholds; i += blockDim.x) {
+                    const int t = i & (kPadThresholds - 1);
+                    s_thr[i] = t < T ? g_thr[(i >> 5) * T + t] : INFINITY;
+                }
+            } else {
+                for (int i = tid; i < nf * T; i += blockDim.x) s_thr[i] = g_thr[i];
             }
+            for (int i = tid; i < nf * T; i += blockDim.x) s_rank[i] = a.ranks[static_cast<long long>(f0) * T + i];
             const int nbins = nf * cp * T1;
             for (int i = tid; i < nbins; i += blockDim.x) s_bins[i] = 0u;
             __syncthreads();
 
             const int W = a.ds.width, H = a.ds.height;
-            if (N >= static_cast<int>(blockDim.x)) {
-                // ---- histogram, sample-major: each thread keeps one sample and walks the tile's
-                // features, so the sample's neighbourhood is reused from L1 across features
-                for (int s0 = 0; s0 < N; s0 += blockDim.x) {
-                    const int s = s0 + tid;
-                    const bool valid = s < N;
-                    EvalPixel px;
-                    int lid = 0, flip = 0;
-                    if (valid) {
-                        const Sample smp = a.samples[nd.start + s];
-                        px = make_eval_pixel(a.ds, smp);
-                        lid = s_lid[smp.label];
-                        flip = smp.flip;
-                    }
-                    const bool any_both = __any_sync(kFull, flip == 2);
-                    // two features per step: their evaluations are independent, so their gathers and
-                    // arithmetic overlap before the two warp-synchronous increments
-                    int f = 0;
-                    for (; f + 1 < nf; f += 2) {
-                        const EvalFeat& fa = s_params[f];
-                        const EvalFeat& fb = s_params[f + 1];
-                        const int row_a = (f * cp + lid) * T1;
-                        const int row_b = ((f + 1) * cp + lid) * T1;
-                        const int ka = valid ? row_a + feature_bin(px, W, H, fa, flip == 1, s_thr + f * T, T) : -1;
-                        const int kb =
-                            valid ? row_b + feature_bin(px, W, H, fb, flip == 1, s_thr + (f + 1) * T, T) : -1;
-                        bin_increment<kAgg>(s_bins, ka);
-                        bin_increment<kAgg>(s_bins, kb);
-                        if (any_both) {
-                            const int ka2 = flip == 2 ? row_a + feature_bin(px, W, H, fa, true, s_thr + f * T, T) : -1;
-                            const int kb2 =
-                                flip == 2 ? row_b + feature_bin(px, W, H, fb, true, s_thr + (f + 1) * T, T) : -1;
-                            bin_increment<kAgg>(s_bins, ka2);
-                            bin_increment<kAgg>(s_bins, kb2);
-                        }
-                    }
-                    if (f < nf) {
-                        const EvalFeat& fp = s_params[f];
-                        const float* sorted = s_thr + f * T;
-                        const int row = (f * cp + lid) * T1;
-                        const int key1 = valid ? row + feature_bin(px, W, H, fp, flip == 1, sorted, T) : -1;
-                        bin_increment<kAgg>(s_bins, key1);
-                        if (any_both) {
-                            const int key2 = flip == 2 ? row + feature_bin(px, W, H, fp, true, sorted, T) : -1;
-                            bin_increment<kAgg>(s_bins, key2);
-                        }
+            const int nthr = blockDim.x;
+            const int n_major = (N / nthr) * nthr;
+            // ---- histogram, sample-major over whole blocks of samples: each thread keeps one sample
+            // and walks the tile's features, so the sample's neighbourhood is reused from L1
+            for (int s0 = 0; s0 < n_major; s0 += nthr) {
+                const Sample smp = a.samples[nd.start + s0 + tid];
+                const EvalPixel px = make_eval_pixel(a.ds, smp);
+                const int lid = s_lid[smp.label];
+                const int flip = smp.flip;
+                const bool any_both = __any_sync(kFull, flip == 2);
+                // two features per step: their evaluations are independent, so their gathers and
+                // arithmetic overlap before the two warp-synchronous increments
+                int f = 0;
+                for (; f + 1 < nf; f += 2) {
+                    const EvalFeat& fa = s_params[f];
+                    const EvalFeat& fb = s_params[f + 1];
+                    const float* sa = s_thr + f * TP;
+                    const float* sb = sa + TP;
+                    const int row_a = (f * cp + lid) * T1;
+                    const int row_b = row_a + cp * T1;
+                    const int ka = row_a + feature_bin<kPad32>(px, W, H, fa, flip == 1, sa, T);
+                    const int kb = row_b + feature_bin<kPad32>(px, W, H, fb, flip == 1, sb, T);
+                    bin_increment<kAgg>(s_bins, ka);
+                    bin_increment<kAgg>(s_bins, kb);
+                    if (any_both) {
+                        const int ka2 = flip == 2 ? row_a + feature_bin<kPad32>(px, W, H, fa, true, sa, T) : -1;
+                        const int kb2 = flip == 2 ? row_b + feature_bin<kPad32>(px, W, H, fb, true, sb, T) : -1;
+                        bin_increment<kAgg>(s_bins, ka2);
+                        bin_increment<kAgg>(s_bins, kb2);
                     }
                 }
-            } else {
-                // ---- histogram, pair-major for small nodes: pairs p = f * N + s, uniform trip count
-                // so warps stay converged
-                const long long pairs = static_cast<long long>(nf) * N;
-                const int iters = static_cast<int>((pairs + blockDim.x - 1) / blockDim.x);
-                const int stride = blockDim.x;
-                const int qstep = stride / N;
-                const int rstep = stride - qstep * N;
-                int f = tid / N;
-                int s = tid - f * N;
+                if (f < nf) {
+                    const EvalFeat& fp = s_params[f];
+                    const float* sorted = s_thr + f * TP;
+                    const int row = (f * cp + lid) * T1;
+                    const int key1 = row + feature_bin<kPad32>(px, W, H, fp, flip == 1, sorted, T);
+                    bin_increment<kAgg>(s_bins, key1);
+                    if (any_both) {
+                        const int key2 = flip == 2 ? row + feature_bin<kPad32>(px, W, H, fp, true, sorted, T) : -1;
+                        bin_increment<kAgg>(s_bins, key2);
+                    }
+                }
+            }
+            // ---- the remaining Nt < blockDim samples, pair-major: pairs p = f * Nt + s spread over
+            // all threads with a uniform trip count so warps stay converged
+            const int Nt = N - n_major;
+            if (Nt > 0) {
+                const Sample* tail = a.samples + nd.start + n_major;
+                const long long pairs = static_cast<long long>(nf) * Nt;
+                const int iters = static_cast<int>((pairs + nthr - 1) / nthr);
+                const int qstep = nthr / Nt;
+                const int rstep = nthr - qstep * Nt;
+                int f = tid / Nt;
+                int s = tid - f * Nt;
                 for (int it = 0; it < iters; it++) {
                     int key1 = -1, key2 = -1;
                     if (f < nf) {
-                        const Sample smp = a.samples[nd.start + s];
+                        const Sample smp = tail[s];
                         const EvalPixel px = make_eval_pixel(a.ds, smp);
                         const EvalFeat& fp = s_params[f];
-                        const float* sorted = s_thr + f * T;
+                        const float* sorted = s_thr + f * TP;
                         const int row = (f * cp + s_lid[smp.label]) * T1;
-                        key1 = row + feature_bin(px, W, H, fp, smp.flip == 1, sorted, T);
-                        if (smp.flip == 2) key2 = row + feature_bin(px, W, H, fp, true, sorted, T);
+                        key1 = row + feature_bin<kPad32>(px, W, H, fp, smp.flip == 1, sorted, T);
+                        if (smp.flip == 2) key2 = row + feature_bin<kPad32>(px, W, H, fp, true, sorted, T);
                     }
                     bin_increment<kAgg>(s_bins, key1);
                     if (__any_sync(kFull, key2 >= 0)) bin_increment<kAgg>(s_bins, key2);
                     s += rstep;
                     f += qstep;
-                    if (s >= N) {
-                        s -= N;
+                    if (s >= Nt) {
+                        s -= Nt;
                         f++;
                     }
                 }
@@ -366,10 +371,10 @@ level_eval_kernel(EvalArgs a) {
                             int pos = s_cn;
                             while (pos > 0 && static_cast<long long>(s_ct[pos - 1]) * a.F + s_cf[pos - 1] > key) pos--;
                             if (pos >= kMaxCand) {
-                                s_ovf = 1;
+                                s_drop = fmax(s_drop, s_scores[ii]);
                                 continue;
                             }
-                            if (s_cn == kMaxCand) s_ovf = 1;
+                            if (s_cn == kMaxCand) s_drop = fmax(s_drop, s_cs[kMaxCand - 1]);
                             const int last = min(s_cn, kMaxCand - 1);
                             for (int j = last; j > pos; j--) {
                                 s_cs[j] = s_cs[j - 1];
@@ -392,7 +397,8 @@ level_eval_kernel(EvalArgs a) {
             ItemCandidates c;
             c.best = s_best;
             c.n = s_cn;
-            c.overflow = s_ovf;
+            c.pad = 0;
+            c.dropped = s_drop;
             for (int j = 0; j < kMaxCand; j++) {
                 c.s[j] = j < s_cn ? s_cs[j] : -INFINITY;
                 c.t[j] = j < s_cn ? s_ct[j] : 0;
@@ -411,11 +417,9 @@ __global__ void reduce_candidates_kernel(int M, int F, const int* __restrict__ i
     if (node >= M) return;
     const int b = item_range[node], e = item_range[node + 1];
     double m = -INFINITY;
+    for (int i = b; i < e; i++) m = fmax(m, cands[i].best);
     int ovf = 0;
-    for (int i = b; i < e; i++) {
-        m = fmax(m, cands[i].best);
-        ovf |= cands[i].overflow;
-    }
+    for (int i = b; i < e; i++) ovf |= __dsub_rn(m, cands[i].dropped) < 1e-13 ? 1 : 0;
     long long best_key = LLONG_MAX;
     double best_s = m;
     int bt = 0, bf = 0;
@@ -530,7 +534,106 @@ __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const 
     scores[static_cast<long long>(thresh) * F + feature] = score;
 }
 
+// Shared-memory layout of a level_eval launch; budget = histogram words (at least one feature).
+SmemLayout level_eval_smem(int C, int T, const EvalTuning& tuning, int* budget) {
+    *budget = std::max(tuning.bins_budget_words, C * (T + 1));
+    const int TP = T < kPadThresholds ? kPadThresholds : T;
+    return SmemLayout(C, T, TP, tuning.ft_max, *budget);
+}
+
+// Shared-memory carveout (percent of the SM's 228 KB) that just holds `ctas` CTAs of `smem` dynamic
+// bytes (+ static shared memory and the 1 KB the runtime reserves per CTA); the rest of the unified
+// 256 KB stays L1, which caches the integral-image gathers.
+template <typename K>
+void set_level_eval_smem(K kernel, size_t smem, int ctas) {
+    cudaFuncAttributes fa;
+    CF_CUDA_CHECK(cudaFuncGetAttributes(&fa, kernel));
+    CF_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    const double need = static_cast<double>(ctas) * (smem + fa.sharedSizeBytes + 1024);
+    const int pct = std::min(100, static_cast<int>(std::ceil(100.0 * need / (228.0 * 1024))));
+    CF_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+}
+
+template <bool kAgg, bool kPad32>
+void launch_level_eval_t(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm) {
+    if (ctas_per_sm >= 4) {
+        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 4>, smem, ctas_per_sm);
+        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 4>, args);
+    } else {
+        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 3>, smem, ctas_per_sm);
+        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 3>, args);
+    }
+}
+
+// The level_eval instance for the tuning and threshold count (T <= 31 takes the padded search).
+void launch_level_eval(cf_context* ctx, const EvalArgs& args, int grid, const EvalTuning& tuning) {
+    int budget = 0;
+    const SmemLayout lay = level_eval_smem(args.C, args.T, tuning, &budget);
+    CF_REQUIRE(lay.total + 4096 <= ctx->smem_per_block_optin,
+               "split search: classes x thresholds too large for shared memory");
+    CF_REQUIRE(args.bins_budget == budget && args.ft_max == tuning.ft_max, "split search: inconsistent tuning");
+    const bool pad = args.T < kPadThresholds;
+    if (tuning.warp_aggregate) {
+        if (pad) launch_level_eval_t<true, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
+        else launch_level_eval_t<true, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
+    } else {
+        if (pad) launch_level_eval_t<false, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
+        else launch_level_eval_t<false, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
+    }
+}
+
 }  // namespace
+
+EvalTuning EvalTuning::of(cf_context* ctx) {
+    cf_eval_tuning t;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        t = ctx->tuning;
+    }
+    EvalTuning e;
+    e.ft_max = t.features_per_tile;
+    e.bins_budget_words = t.bins_budget_words;
+    e.warp_aggregate = t.warp_aggregate;
+    e.ctas_per_sm = t.ctas_per_sm;
+    e.items_per_slot = t.items_per_slot;
+    e.feature_granule = t.feature_granule;
+    return e;
+}
+
+void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
+                      std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order) {
+    const int M = static_cast<int>(node_counts.size());
+    const int g = std::max(1, tuning.feature_granule);
+    long long total_work = 0;
+    for (int n : node_counts) total_work += static_cast<long long>(n) * F;
+    const double target_items = tuning.items_per_slot * slots;
+    const double work_per_item = std::max(1.0, static_cast<double>(total_work) / target_items);
+    items.clear();
+    range.assign(M + 1, 0);
+    std::vector<long long> work;
+    for (int n = 0; n < M; n++) {
+        range[n] = static_cast<int>(items.size());
+        const double w = static_cast<double>(node_counts[n]) * F;
+        int parts = static_cast<int>(std::ceil(w / work_per_item));
+        parts = std::max(1, std::min(parts, (F + g - 1) / g));
+        int per = (F + parts - 1) / parts;
+        per = ((per + g - 1) / g) * g;
+        for (int f0 = 0; f0 < F; f0 += per) {
+            EvalItem it;
+            it.node = n;
+            it.f_begin = f0;
+            it.f_end = std::min(F, f0 + per);
+            it.pad = 0;
+            items.push_back(it);
+            work.push_back(static_cast<long long>(node_counts[n]) * (it.f_end - it.f_begin));
+        }
+    }
+    range[M] = static_cast<int>(items.size());
+    const int n_items = static_cast<int>(items.size());
+    order.resize(n_items);
+    for (int i = 0; i < n_items; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+}
 
 // ------------------------------------------------------------------------------------------------
 void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
@@ -540,37 +643,10 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     CF_REQUIRE(C >= 1 && C <= 256, "number of classes must be in [1, 256]");
     CF_REQUIRE(T >= 1 && T <= 4096, "number of thresholds must be in [1, 4096]");
     if (M == 0) return;
-    // work items: feature ranges sized so that the level yields ~items_per_slot items per resident CTA
-    long long total_work = 0;
-    for (int n : node_counts) total_work += static_cast<long long>(n) * F;
+    tuning = EvalTuning::of(ctx);
     const int slots = ctx->num_sms * tuning.ctas_per_sm;
-    const double target_items = tuning.items_per_slot * slots;
-    const double work_per_item = std::max(1.0, static_cast<double>(total_work) / target_items);
-    h_items_.clear();
-    h_range_.assign(M + 1, 0);
-    std::vector<long long> item_work;
-    for (int n = 0; n < M; n++) {
-        h_range_[n] = static_cast<int>(h_items_.size());
-        const double w = static_cast<double>(node_counts[n]) * F;
-        int parts = static_cast<int>(std::ceil(w / work_per_item));
-        parts = std::max(1, std::min(parts, (F + 7) / 8));
-        int per = (F + parts - 1) / parts;
-        per = ((per + 7) / 8) * 8;
-        for (int f0 = 0; f0 < F; f0 += per) {
-            EvalItem it;
-            it.node = n;
-            it.f_begin = f0;
-            it.f_end = std::min(F, f0 + per);
-            it.pad = 0;
-            h_items_.push_back(it);
-            item_work.push_back(static_cast<long long>(node_counts[n]) * (it.f_end - it.f_begin));
-        }
-    }
-    h_range_[M] = static_cast<int>(h_items_.size());
+    plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_);
     const int n_items = static_cast<int>(h_items_.size());
-    h_order_.resize(n_items);
-    for (int i = 0; i < n_items; i++) h_order_[i] = i;
-    std::stable_sort(h_order_.begin(), h_order_.end(), [&](int x, int y) { return item_work[x] > item_work[y]; });
     items_.reserve(n_items);
     order_.reserve(n_items);
     item_range_.reserve(M + 1);
@@ -585,11 +661,8 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int), ctx->stream));
     last_items = n_items;
 
-    int budget = tuning.bins_budget_words;
-    budget = std::max(budget, C * (T + 1));
-    const SmemLayout lay(C, T, tuning.ft_max, budget);
-    CF_REQUIRE(lay.total + 4096 <= ctx->smem_per_block_optin,
-               "split search: classes x thresholds too large for shared memory");
+    int budget = 0;
+    level_eval_smem(C, T, tuning, &budget);
     EvalArgs args;
     args.ds = ds;
     args.samples = samples;
@@ -609,16 +682,7 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     args.ft_max = tuning.ft_max;
     args.bins_budget = budget;
     args.dump_left = dump_left;
-    const int grid = std::min(n_items, slots);
-    if (tuning.warp_aggregate) {
-        CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(lay.total)));
-        launch(ctx, "level_eval", dim3(grid), dim3(256), lay.total, level_eval_kernel<true>, args);
-    } else {
-        CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(lay.total)));
-        launch(ctx, "level_eval", dim3(grid), dim3(256), lay.total, level_eval_kernel<false>, args);
-    }
+    launch_level_eval(ctx, args, std::min(n_items, slots), tuning);
     launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F,
            item_range_.get(), cands_.get(), lf.thr.get(), splits_dev);
 }
@@ -803,37 +867,26 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         const int M = num_nodes, F = num_features, T = num_thresholds, C = num_classes;
         // nodes and work items, sized as the level-batched evaluator sizes them
         std::vector<NodeDesc> nodes(M);
-        long long total_work = 0;
+        std::vector<int> counts(M);
         for (int i = 0; i < M; i++) {
             const long long cnt = node_offsets[i + 1] - node_offsets[i];
             CF_REQUIRE(cnt >= 1 && cnt < (1LL << 31), "cf_evaluate_best_splits_noalloc: every node needs samples");
             nodes[i] = NodeDesc{node_offsets[i], static_cast<int>(cnt), i};
-            total_work += cnt * F;
+            counts[i] = static_cast<int>(cnt);
         }
-        const EvalTuning tuning;
+        EvalTuning tuning = EvalTuning::of(ctx);
         const int slots = ctx->num_sms * tuning.ctas_per_sm;
-        const double work_per_item = std::max(1.0, static_cast<double>(total_work) / (tuning.items_per_slot * slots));
         std::vector<EvalItem> items;
-        std::vector<int> range(M + 1);
-        std::vector<long long> work;
-        for (int n = 0; n < M; n++) {
-            range[n] = static_cast<int>(items.size());
-            int parts = static_cast<int>(std::ceil(static_cast<double>(nodes[n].count) * F / work_per_item));
-            parts = std::max(1, std::min(parts, (F + 7) / 8));
-            int per = (F + parts - 1) / parts;
-            per = ((per + 7) / 8) * 8;
-            for (int f0 = 0; f0 < F; f0 += per) {
-                items.push_back(EvalItem{n, f0, std::min(F, f0 + per), 0});
-                work.push_back(static_cast<long long>(nodes[n].count) * (std::min(F, f0 + per) - f0));
-            }
-            CF_REQUIRE(static_cast<int>(items.size()) <= kNoAllocMaxItems,
-                       "cf_evaluate_best_splits_noalloc: level needs more than 65536 work items");
+        std::vector<int> range, order;
+        // fewer, larger items when the level would need more than the scratch holds
+        for (;;) {
+            plan_level_items(counts, F, tuning, slots, items, range, order);
+            if (items.size() <= static_cast<size_t>(kNoAllocMaxItems) || tuning.items_per_slot < 0.01) break;
+            tuning.items_per_slot *= 0.5;
         }
-        range[M] = static_cast<int>(items.size());
+        CF_REQUIRE(items.size() <= static_cast<size_t>(kNoAllocMaxItems),
+                   "cf_evaluate_best_splits_noalloc: level needs more than 65536 work items");
         const int n_items = static_cast<int>(items.size());
-        std::vector<int> order(n_items);
-        for (int i = 0; i < n_items; i++) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
 
         const NoAllocLayout lay(M, n_items, F, T);
         CF_REQUIRE(lay.total <= kNoAllocScratchBytes, "cf_evaluate_best_splits_noalloc: level too large for the "
@@ -865,10 +918,8 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         ds.width = width;
         ds.height = height;
         ds.plane = static_cast<long long>(width) * height;
-        const int budget = std::max(tuning.bins_budget_words, C * (T + 1));
-        const SmemLayout sl(C, T, tuning.ft_max, budget);
-        CF_REQUIRE(sl.total + 4096 <= ctx->smem_per_block_optin,
-                   "split search: classes x thresholds too large for shared memory");
+        int budget = 0;
+        level_eval_smem(C, T, tuning, &budget);
         EvalArgs args;
         args.ds = ds;
         args.samples = reinterpret_cast<const Sample*>(samples);
@@ -888,9 +939,7 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         args.ft_max = tuning.ft_max;
         args.bins_budget = budget;
         args.dump_left = nullptr;
-        CF_CUDA_CHECK(cudaFuncSetAttribute(level_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(sl.total)));
-        launch(ctx, "level_eval", dim3(std::min(n_items, slots)), dim3(256), sl.total, level_eval_kernel<true>, args);
+        launch_level_eval(ctx, args, std::min(n_items, slots), tuning);
         launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F, d_range,
                d_cands, thresholds, best);
         CF_CUDA_CHECK(cudaStreamSynchronize(st));

@@ -23,24 +23,35 @@ struct EvalItem {
 constexpr int kMaxCand = 4;
 
 // Near-best candidates of one work item: every entry has best - score < 1e-13, sorted by
-// (threshold, feature), at most kMaxCand lowest indices (overflow set when more existed).
+// (threshold, feature), at most kMaxCand lowest indices. `dropped` is the highest score of a
+// candidate that was in the window when a full list pushed it out (-inf if none): the node's
+// choice is exact unless a dropped score lies within the node's final window.
 struct ItemCandidates {
     double best;
     double s[kMaxCand];
     int t[kMaxCand];
     int f[kMaxCand];
     int n;
-    int overflow;
+    int pad;
+    double dropped;
 };
 
+// Launch shape of level_eval (cf_eval_tuning of the context; 256 threads per CTA).
 struct EvalTuning {
-    int threads = 256;
     int ft_max = 32;              // features per tile upper bound
-    int bins_budget_words = 12288;  // shared-memory histogram budget per CTA (u32 words)
+    int bins_budget_words = 7168;   // shared-memory histogram budget per CTA (u32 words)
     int warp_aggregate = 1;       // __match_any_sync aggregation of the shared-memory increments
     int ctas_per_sm = 3;
-    double items_per_slot = 4.0;  // work items per resident CTA for load balance
+    double items_per_slot = 64.0; // work items per resident CTA for load balance
+    int feature_granule = 8;      // a work item covers a multiple of this many features
+
+    static EvalTuning of(cf_context* ctx);
 };
+
+// Work items of one level: node n is cut into feature ranges so that the level yields about
+// items_per_slot items per resident CTA; order lists the items by decreasing work (samples x features).
+void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
+                      std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order);
 
 class LevelEvaluator {
 public:
@@ -49,7 +60,7 @@ public:
     void evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
                   const uint32_t* node_hist_dev, int M, const std::vector<int>& node_counts, int C,
                   const LevelFeatures& lf, cf_split* splits_dev, uint32_t* dump_left = nullptr);
-    EvalTuning tuning;
+    EvalTuning tuning;            // the context's tuning at the last evaluate call
     int64_t last_items = 0;
 
 private:

@@ -53,8 +53,10 @@ typedef struct cf_split {
     int32_t feature;          /* index into the level's sorted candidate table */
     int32_t threshold_index;
     float threshold;
-    int32_t flags;            /* bit 0: more near-ties than the candidate lists hold (argmax exact only
-                                 up to the lowest four indices per work item) */
+    int32_t flags;            /* bit 0: a candidate within 1e-13 of the best score was pushed out of a
+                                 full four-entry candidate list, so the lowest-(threshold, feature)
+                                 tie-break among near-ties is not guaranteed; 0 = exact. Which
+                                 candidates meet in one list depends on the launch shape. */
 } cf_split;
 
 /* TrainingConfiguration (random_tree.h:187-493), the fields the hot path reads. */
@@ -98,6 +100,22 @@ cf_status cf_context_kernel_time(cf_context* ctx, const char* kernel, double* to
 cf_status cf_context_reset_timing(cf_context* ctx);
 /* Number of kernel launches issued by this context since creation. */
 int64_t cf_context_launch_count(cf_context* ctx);
+
+/* Launch shape of the level-batched split search used by every training call on this context.
+ * Project extension with no reference counterpart (the reference's launch shapes are compile-time
+ * constants, random_tree_image_gpu.cu:1455-1720). Read the current values with get, change fields,
+ * write them back with set; set(NULL) restores the defaults. Results do not depend on the tuning,
+ * only speed does. */
+typedef struct cf_eval_tuning {
+    int32_t features_per_tile;   /* features per shared-memory tile at most, 2..64 (default 32) */
+    int32_t bins_budget_words;   /* histogram words per CTA, 1024..49152 (default 7168) */
+    int32_t warp_aggregate;      /* 1: warp-aggregated shared increments (default), 0: plain atomics */
+    int32_t ctas_per_sm;         /* resident CTAs per SM the kernel is compiled for, 1..4 (default 3) */
+    int32_t feature_granule;     /* work items cover a multiple of this many features, 1..64 (default 8) */
+    float items_per_slot;        /* work items per resident CTA, (0, 1024] (default 64) */
+} cf_eval_tuning;
+cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out);
+cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning);
 
 /* ---------------------------------------------------------------------------------------------
  * Datasets: integral images resident in device memory
