@@ -268,6 +268,17 @@ def scores(ctx, counters, node_histogram):
     return out
 
 
+def score_bounds(ctx, counters, node_histogram):
+    """(lower, upper) float32 [T][F] enclosing scores(ctx, counters, node_histogram)."""
+    counters = np.ascontiguousarray(counters, np.uint32)
+    node_histogram = np.ascontiguousarray(node_histogram, np.uint32)
+    F, T, C, _ = counters.shape
+    lo = np.empty((T, F), np.float32)
+    up = np.empty((T, F), np.float32)
+    _check(lib().cf_score_bounds(ctx.handle, C, F, T, _p(counters), _p(node_histogram), _p(lo), _p(up)))
+    return lo, up
+
+
 def generate_features(ds, samples, seed, num_features, num_thresholds, box_radius, region_size, use_depth_images=True):
     samples = np.ascontiguousarray(samples, SAMPLE_DTYPE)
     feats = np.empty((11, num_features), np.int8)

@@ -150,4 +150,76 @@ __device__ __forceinline__ double ig_term(double value, double total, double sid
     return __dmul_rn(p, log2(__ddiv_rn(p, __dmul_rn(sideProb, classProb))));
 }
 
+// ---- float bounds of the score (screening) ----------------------------------------------------
+// With f(x) = x log2 x, the score of a split with left counts l_i, right counts r_i = h_i - l_i,
+// L = sum l_i, R = sum r_i, node total N is, in real arithmetic,
+//     score = 2 S / D,  S = sum f(l_i) + sum f(r_i) - f(L) - f(R) + K,  D = f(N) - f(L) - f(R) + K,
+// K = f(N) - sum f(h_i)  (S = N * information gain, D = N * (H_split + H_classes)).
+// score_bounds evaluates S and D in 2^23-scaled fixed point (below) and widens them by a bound on
+// the log2 error, so the reference's double score lies in [lb, ub]; the widening is far above the
+// rounding error of the reference's own double evaluation. Where D may be tiny relative to N the
+// bounds are [0, 1].
+struct ScoreConsts {
+    double fN;      // f(N)
+    double K;       // f(N) - sum f(h_i)
+    double Nd;      // N
+    uint32_t N;
+};
+
+// round(2^23 x log2 x) up to x (2^-22 + 2^-23) 2^23: with float(x) = m 2^e, m in [1, 2),
+// x log2 x ~ x (e + log2 m); e is exact, __log2f(m) has absolute error <= 2^-22 on [1, 2], its 23
+// fraction bits are rounded (2^-24) and float(x) is rounded for x > 2^24 (x log2(1 + 2^-24) <
+// 1.5 x 2^-24). The product x * (e 2^23 + frac) < 2^60 is exact in 64-bit integers, so sums of
+// these terms carry no rounding error at all.
+__device__ __forceinline__ long long xlog2x_fixed(uint32_t x) {
+    const uint32_t b = __float_as_uint(__uint2float_rn(x));
+    const uint32_t e = (b >> 23) - 127u;
+    const float lg = fmaxf(__log2f(__uint_as_float((b & 0x7FFFFFu) | 0x3F800000u)), 0.0f);
+    const uint32_t frac = __float_as_uint(lg + 1.0f) - 0x3F800000u;   // round(2^23 lg), <= 2^23
+    const unsigned long long p = static_cast<unsigned long long>(x) * ((e << 23) + frac);
+    return x == 0u ? 0LL : static_cast<long long>(p);
+}
+
+__device__ __forceinline__ ScoreConsts score_consts(const uint32_t* counts, int n) {
+    double N = 0, sum_fh = 0;
+    for (int i = 0; i < n; i++) {
+        const double h = static_cast<double>(counts[i]);
+        N += h;
+        if (h > 0) sum_fh += h * log2(h);
+    }
+    ScoreConsts k;
+    k.fN = N > 0 ? N * log2(N) : 0.0;
+    k.K = k.fN - sum_fh;
+    k.Nd = N;
+    k.N = static_cast<uint32_t>(N);
+    return k;
+}
+
+// (lb, ub) of the score; left(i) = left count of class i (i < n), counts[i] = h_i.
+template <typename LeftCount>
+__device__ __forceinline__ float2 score_bounds(LeftCount left, const uint32_t* counts, int n, const ScoreConsts& k) {
+    uint32_t L = 0;
+    long long acc = 0;
+    for (int i = 0; i < n; i++) {
+        const uint32_t l = left(i);
+        L += l;
+        acc += xlog2x_fixed(l) + xlog2x_fixed(counts[i] - l);
+    }
+    const uint32_t R = k.N - L;
+    if (L == 0u || R == 0u) return make_float2(0.0f, 0.0f);   // the reference scores 0
+    const long long fLR = xlog2x_fixed(L) + xlog2x_fixed(R);
+    const double S = static_cast<double>(acc - fLR) * 0x1p-23 + k.K;    // N * information gain
+    const double D = k.fN - static_cast<double>(fLR) * 0x1p-23 + k.K;   // N * (H_split + H_classes)
+    // every x of the sum of l_i, r_i terms (2N in total) and of L, R (N) contributes
+    // <= 0.75 x 2^-21; 2^-19 N covers S and D with room for the products' and sums' roundings
+    const double e = 0x1p-19 * k.Nd;
+    const float dlo = static_cast<float>(D - e);
+    if (!(dlo > 1e-4f * static_cast<float>(k.Nd))) return make_float2(0.0f, 1.0f);
+    float ub = 2.0f * static_cast<float>(S + e) / dlo;
+    float lb = 2.0f * static_cast<float>(S - e) / static_cast<float>(D + e);
+    ub = fminf(1.0f, fmaxf(0.0f, ub * 1.0000038f + 1e-8f));   // (1 + 2^-18), covers the float ops above
+    lb = fminf(1.0f, fmaxf(0.0f, lb * 0.9999962f - 1e-8f));
+    return make_float2(lb, ub);
+}
+
 }  // namespace cf

@@ -135,6 +135,8 @@ level_eval_kernel(EvalArgs a) {
     __shared__ int s_warp_cnt[8];
     __shared__ int s_cp;
     __shared__ double s_total, s_hc;
+    __shared__ ScoreConsts s_k;
+    __shared__ float s_wmax[8];
     __shared__ double s_best;
     __shared__ double s_cs[kMaxCand];
     __shared__ int s_ct[kMaxCand], s_cf[kMaxCand];
@@ -195,9 +197,11 @@ level_eval_kernel(EvalArgs a) {
                 for (int i = 0; i < s_cp; i++) total += static_cast<double>(s_counts[i]);
                 s_total = total;
                 s_hc = classification_entropy(s_cp, s_counts, total);
+                s_k = score_consts(s_counts, s_cp);
             }
             __syncthreads();
         }
+        const ScoreConsts sk = s_k;
         const int cp = s_cp;
         const double total = s_total;
         const double hc = s_hc;
@@ -325,12 +329,37 @@ level_eval_kernel(EvalArgs a) {
                 }
             }
 
-            // ---- scores of every (feature, threshold) of the tile
-            for (int i = tid; i < nf * T; i += blockDim.x) {
-                const int fl = i / T;
-                const int t = i - fl * T;
-                const int rank = s_rank[fl * T + t];
-                s_scores[i] = score_from_cum(s_bins + fl * cp * T1 + rank, T1, s_counts, cp, total, hc);
+            // ---- scores of the tile: float bounds for every (feature, threshold) first; the exact
+            // double score only where the upper bound reaches the 1e-13 window below the best lower
+            // bound (or the item's best so far). A pair left out cannot be within the window of the
+            // final best, so the candidates and the chosen split are those of scoring every pair.
+            {
+                float2* s_bounds = reinterpret_cast<float2*>(s_scores);   // slot i: (lb, ub), then the score
+                float lbmax = 0.0f;
+                for (int i = tid; i < nf * T; i += blockDim.x) {
+                    const int fl = i / T;
+                    const int t = i - fl * T;
+                    const uint32_t* cum = s_bins + fl * cp * T1 + s_rank[fl * T + t];
+                    const float2 b = score_bounds([&](int c) { return cum[c * T1]; }, s_counts, cp, sk);
+                    s_bounds[i] = b;
+                    lbmax = fmaxf(lbmax, b.x);
+                }
+                for (int off = 16; off > 0; off >>= 1) lbmax = fmaxf(lbmax, __shfl_xor_sync(kFull, lbmax, off));
+                if (lane == 0) s_wmax[warp] = lbmax;
+                __syncthreads();
+                float m = s_wmax[0];
+                for (int w = 1; w < static_cast<int>(blockDim.x >> 5); w++) m = fmaxf(m, s_wmax[w]);
+                const double floor_s = fmax(static_cast<double>(m), s_best) - 1e-13;
+                for (int i = tid; i < nf * T; i += blockDim.x) {
+                    const float ub = s_bounds[i].y;
+                    double sc = -INFINITY;
+                    if (static_cast<double>(ub) >= floor_s) {
+                        const int fl = i / T;
+                        const int t = i - fl * T;
+                        sc = score_from_cum(s_bins + fl * cp * T1 + s_rank[fl * T + t], T1, s_counts, cp, total, hc);
+                    }
+                    s_scores[i] = sc;
+                }
             }
             __syncthreads();
 
@@ -489,6 +518,21 @@ __global__ void plain_histogram_kernel(const double* __restrict__ resp1, const d
 }
 
 // scoreKernel: one thread per (threshold, feature); scores [T][F]
+// Float score bounds [T][F] from counters [F][T][C][2] (the level kernel's screening, standalone).
+__global__ void score_bounds_kernel(const uint32_t* __restrict__ counters, const uint32_t* __restrict__ hist, int C,
+                                    int F, int T, float* __restrict__ lower, float* __restrict__ upper) {
+    __shared__ ScoreConsts s_k;
+    if (threadIdx.x == 0) s_k = score_consts(hist, C);
+    __syncthreads();
+    const int feature = blockIdx.x * blockDim.x + threadIdx.x;
+    const int thresh = blockIdx.y;
+    if (feature >= F) return;
+    const uint32_t* lr = counters + (static_cast<long long>(feature) * T + thresh) * C * 2;
+    const float2 b = score_bounds([&](int c) { return lr[2 * c]; }, hist, C, s_k);
+    lower[static_cast<long long>(thresh) * F + feature] = b.x;
+    upper[static_cast<long long>(thresh) * F + feature] = b.y;
+}
+
 __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const uint32_t* __restrict__ hist, int C, int F,
                                    int T, double* __restrict__ scores) {
     __shared__ double s_hc;
@@ -701,6 +745,13 @@ void plain_scores(cf_context* ctx, int C, int F, int T, const uint32_t* counters
     const int tpb = std::min(F, 128);
     launch(ctx, "plain_score", dim3((F + tpb - 1) / tpb, T), dim3(tpb), 0, plain_score_kernel, counters, node_hist, C,
            F, T, scores);
+}
+
+void score_bounds(cf_context* ctx, int C, int F, int T, const uint32_t* counters, const uint32_t* node_hist,
+                  float* lower, float* upper) {
+    const int tpb = std::min(F, 128);
+    launch(ctx, "score_bounds", dim3((F + tpb - 1) / tpb, T), dim3(tpb), 0, score_bounds_kernel, counters, node_hist,
+           C, F, T, lower, upper);
 }
 
 void PlainNodeEvaluator::histograms(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start,

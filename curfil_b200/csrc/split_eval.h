@@ -92,6 +92,9 @@ public:
 
 void plain_responses(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start, int count,
                      const int8_t* feat_table, int F, double* resp1, double* resp2);
+// Float bounds [T][F] of the exact scores (the screening of level_eval), counters [F][T][C][2].
+void score_bounds(cf_context* ctx, int C, int F, int T, const uint32_t* counters, const uint32_t* node_hist,
+                  float* lower, float* upper);
 void plain_scores(cf_context* ctx, int C, int F, int T, const uint32_t* counters, const uint32_t* node_hist,
                   double* scores);
 

@@ -339,6 +339,36 @@ cf_status cf_scores(cf_context* ctx, int num_classes, int num_features, int num_
     });
 }
 
+cf_status cf_score_bounds(cf_context* ctx, int num_classes, int num_features, int num_thresholds,
+                          const uint32_t* counters, const uint32_t* node_histogram, float* lower, float* upper) {
+    return guard([&] {
+        CF_REQUIRE(ctx && counters && node_histogram && lower && upper, "cf_score_bounds: NULL argument");
+        CF_REQUIRE(num_classes >= 1 && num_classes <= 256 && num_features > 0 && num_thresholds > 0,
+                   "cf_score_bounds: empty input or more than 256 classes");
+        make_current(ctx);
+        const size_t nc = static_cast<size_t>(num_features) * num_thresholds * num_classes * 2;
+        const size_t ns = static_cast<size_t>(num_features) * num_thresholds;
+        for (size_t i = 0; i < nc; i += 2) {
+            const size_t c = (i / 2) % num_classes;
+            CF_REQUIRE(static_cast<uint64_t>(counters[i]) + counters[i + 1] == node_histogram[c],
+                       "cf_score_bounds: left + right counts must equal the node histogram");
+        }
+        DevArray<uint32_t> c, h;
+        DevArray<float> lo, up;
+        c.reserve(nc);
+        h.reserve(num_classes);
+        lo.reserve(ns);
+        up.reserve(ns);
+        CF_CUDA_CHECK(cudaMemcpyAsync(c.get(), counters, sizeof(uint32_t) * nc, cudaMemcpyHostToDevice, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(h.get(), node_histogram, sizeof(uint32_t) * num_classes, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        score_bounds(ctx, num_classes, num_features, num_thresholds, c.get(), h.get(), lo.get(), up.get());
+        CF_CUDA_CHECK(cudaMemcpyAsync(lower, lo.get(), sizeof(float) * ns, cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaMemcpyAsync(upper, up.get(), sizeof(float) * ns, cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
 cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample* samples, uint32_t seed,
                                int num_features, int num_thresholds, int box_radius, int region_size,
                                int use_depth_images, int8_t* features, float* thresholds) {

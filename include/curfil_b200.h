@@ -152,6 +152,11 @@ cf_status cf_histograms(cf_dataset* ds, int num_samples, const cf_sample* sample
  * [F][T][C][2] and the node histogram [C]. */
 cf_status cf_scores(cf_context* ctx, int num_classes, int num_features, int num_thresholds,
                     const uint32_t* counters, const uint32_t* node_histogram, double* scores);
+/* Float lower/upper bounds [T][F] that enclose the scores cf_scores returns for the same counters
+ * (left + right must equal the node histogram per class). Project extension with no reference
+ * counterpart: the screening the level-batched split search applies before exact double scoring. */
+cf_status cf_score_bounds(cf_context* ctx, int num_classes, int num_features, int num_thresholds,
+                          const uint32_t* counters, const uint32_t* node_histogram, float* lower, float* upper);
 /* generateRandomFeatures (random_tree_image_gpu.cu:1896-1956 + sortFeatures :1853-1894): the
  * candidate generator of the GPU path on a Philox4x32-10 stream, sorted by getSortKey. */
 cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample* samples, uint32_t seed,
