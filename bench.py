@@ -16,6 +16,7 @@ Under torchrun every rank trains its own trees (trees are independent; no collec
 import argparse
 import json
 import os
+import queue
 import statistics
 import subprocess
 import sys
@@ -28,7 +29,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W = dict(images=200, width=640, height=480, cells=40, classes=40, samples_per_image=4000, trees=3, max_depth=20,
-         features=2000, thresholds=20, min_samples=50, box_radius=60, region_size=15, predict_images=50, seed=2026)
+         features=2000, thresholds=20, min_samples=50, box_radius=60, region_size=15, predict_images=64,
+         predict_trees=10, seed=2026)
+# serving: Poisson arrivals of mixed frame sizes (weights 1:2:4:1) at these offered rates
+SERVE_RATES = (200, 1000, 4000)
+SERVE_SIZES = ((160, 120, 1), (320, 240, 2), (640, 480, 4), (1280, 960, 1))
 BYTES_DEPTH_EVAL = 64   # 2 boxes x 4 corners x (int32 depth sum + int32 valid count)
 BYTES_COLOR_EVAL = 32   # 2 boxes x 4 corners x float32
 METRIC = "train feature-evals/s"
@@ -194,6 +199,147 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------------------- prediction
+def forest_trees(ds, labels, depth, cfg, n_trees):
+    """n_trees trees trained with the full-size settings, the forest sampling split over n_trees."""
+    import curfil_b200 as cf
+    seed = cf.forest_seed(cfg.random_seed)
+    trees = []
+    for t in range(n_trees):
+        s, prior, counter = cf.sample_tree_pixels(labels, depth, W["classes"], cfg, n_trees, seed + t)
+        tree, _ = cf.train_tree(ds, s, W["classes"], cfg, tree_id=t, seed_counter=counter)
+        tree.set_prior(prior)
+        trees.append(tree)
+    return trees
+
+
+def predict_section(ctx, stream, ds, trees, local, serve_seconds):
+    """Batch prediction of resident frames (one launch), the plain per-image launch form on the same
+    frames (identical results required), a CUDA-graph replay from pinned host frames, and Poisson
+    serving of mixed frame sizes."""
+    import torch
+    import curfil_b200 as cf
+    n, C, H, Wd = W["predict_images"], W["classes"], W["height"], W["width"]
+    px = n * H * Wd
+    forest = cf.Forest(ctx, trees)
+    out = {"images": n, "frame": "%dx%d" % (Wd, H), "trees": len(trees), "forest_nodes": forest.num_nodes}
+    pa = torch.empty((n, C, H, Wd), dtype=torch.float32, device=local)
+    la = torch.empty((n, H, Wd), dtype=torch.uint8, device=local)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ctx.reset_timing()
+    ctx.set_timing(True)
+    ms = timed(lambda: forest.predict_dataset(ds, 0, n, pa.data_ptr(), la.data_ptr()), 5)
+    ctx.set_timing(False)
+    k_ms, k_n = ctx.kernel_time("classify")
+    peak, peak_kind = load_peaks()
+    bpp = 20 + 4 * C + 1   # integral images (colour 12 B + depth 8 B) read, probabilities and label written
+    achieved = px * bpp / (k_ms / k_n / 1e3) / 1e9
+    out["batched"] = {"mpx_per_s": px / (ms / 1e3) / 1e6, "ms_per_batch": ms, "ms_per_frame": ms / n,
+                      "roofline": {"bound": "hbm", "kernel": "classify", "achieved": achieved, "peak": peak,
+                                   "unit": "GB/s", "frac": achieved / peak, "bytes_per_px": bpp,
+                                   "avg_launch_ms": k_ms / k_n, "peak_source": peak_kind}}
+    pb = torch.empty_like(pa)
+    lb = torch.empty_like(la)
+    pms = timed(lambda: forest.predict_dataset_plain(ds, 0, n, pb.data_ptr(), lb.data_ptr()), 1)
+    out["plain_per_image"] = {"mpx_per_s": px / (pms / 1e3) / 1e6, "ms_per_frame": pms / n,
+                              "note": "one launch + synchronisation per tree per image, then normalise and argmax"}
+    out["speedup_vs_plain"] = pms / ms
+    out["labels_identical"] = bool(torch.equal(la, lb))
+    out["probabilities_identical"] = bool(torch.equal(pa.view(torch.int32), pb.view(torch.int32)))
+    del pa, la, pb, lb
+
+    # the same 64 frames from pinned host buffers through one CUDA graph replay (labels back to the host)
+    rgb, depth, _ = cf.synthetic_frames(W["seed"] + 7, n, Wd, H, W["cells"], C)
+    g = cf.PredictGraph(forest, n, Wd, H, probabilities=False)
+    g.rgb[...] = rgb
+    g.depth[...] = depth
+    g.run()
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        g.run()
+    gs = (time.perf_counter() - t0) / reps
+    out["graph_e2e"] = {"mpx_per_s": px / gs / 1e6, "ms_per_batch": gs * 1e3,
+                        "h2d_bytes_per_batch": int(rgb.nbytes + depth.nbytes), "d2h_bytes_per_batch": int(px),
+                        "note": "pinned host RGB-D -> H2D -> integral images -> classify -> labels D2H, one graph"}
+    g.close()
+    if serve_seconds > 0:
+        out["serving"] = serve(forest, serve_seconds)
+    forest.close()
+    return out
+
+
+def serve(forest, seconds):
+    """Poisson arrivals (seeded) at each offered rate, frame sizes 160x120 : 320x240 : 640x480 :
+    1280x960 = 1:2:4:1; latency = completion - submission on the server's clock."""
+    import curfil_b200 as cf
+    pool = {}
+    for w, h, _ in SERVE_SIZES:
+        rgb, depth, _ = cf.synthetic_frames(W["seed"] + w, 4, w, h, W["cells"], W["classes"])
+        pool[(w, h)] = (rgb, depth)
+    weights = np.array([k for _, _, k in SERVE_SIZES], np.float64)
+    results = []
+    for rate in SERVE_RATES:
+        rng = np.random.default_rng(rate)
+        count = max(8, int(rate * seconds))
+        gaps = rng.exponential(1.0 / rate, count)
+        kinds = rng.choice(len(SERVE_SIZES), count, p=weights / weights.sum())
+        which = rng.integers(0, 4, count)
+        srv = cf.Server(forest, hbm_budget_bytes=8 << 30, max_batch_frames=32, max_pending=1 << 16, pipeline_depth=3)
+        # warm the server with one frame of each size
+        for w, h, _ in SERVE_SIZES:
+            rgb, depth = pool[(w, h)]
+            srv.wait(srv.submit(rgb[0], depth[0]), (h, w))
+        ids = []
+        done = {}
+
+        def drain():
+            for rid, shape in iter(q.get, None):
+                _, _, st = srv.wait(rid, shape, timeout_s=60.0)
+                done[rid] = (st.submit_ms, st.admitted_ms, st.done_ms, shape)
+
+        q = queue.Queue()
+        waiter = threading.Thread(target=drain)
+        waiter.start()
+        t = time.perf_counter()
+        for i in range(count):
+            t += gaps[i]
+            while time.perf_counter() < t:
+                pass
+            w, h, _ = SERVE_SIZES[kinds[i]]
+            rgb, depth = pool[(w, h)]
+            rid = srv.submit(rgb[which[i]], depth[which[i]])
+            ids.append(rid)
+            q.put((rid, (h, w)))
+        q.put(None)
+        waiter.join()
+        lat = np.array([done[r][2] - done[r][0] for r in ids])
+        qwait = np.array([done[r][1] - done[r][0] for r in ids])
+        big = np.array([done[r][3] == (480, 640) for r in ids])
+        span = (max(done[r][2] for r in ids) - min(done[r][0] for r in ids)) / 1e3
+        pxs = sum(done[r][3][0] * done[r][3][1] for r in ids)
+        c = srv.counters()
+        srv.close()
+        results.append({"offered_fps": rate, "frames": count, "offered_mpx_per_s": rate * pxs / count / 1e6,
+                        "mpx_per_s": pxs / span / 1e6, "p50_ms": float(np.percentile(lat, 50)),
+                        "p99_ms": float(np.percentile(lat, 99)),
+                        "p99_ms_640x480": float(np.percentile(lat[big], 99)) if big.any() else None,
+                        "p99_admission_wait_ms": float(np.percentile(qwait, 99)),
+                        "batches": c["batches"] - len(SERVE_SIZES), "rejected": c["rejected"]})
+    return {"sizes": "160x120:320x240:640x480:1280x960 = 1:2:4:1", "trees": forest.num_trees, "rates": results}
+
+
 # ----------------------------------------------------------------------------------------- our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -203,16 +349,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-per-node", action="store_true", help="skip the plain per-node comparison tree")
     # workload size (defaults: the full-size configuration); smaller cases are for profiler captures
     ap.add_argument("--images", type=int, default=W["images"])
     ap.add_argument("--trees", type=int, default=W["trees"])
     ap.add_argument("--max-depth", type=int, default=W["max_depth"])
     ap.add_argument("--predict-images", type=int, default=W["predict_images"])
+    ap.add_argument("--predict-trees", type=int, default=W["predict_trees"])
+    ap.add_argument("--serve-seconds", type=float, default=1.5, help="Poisson load per offered rate (0: skip)")
     ap.add_argument("--tuning", default="", help="split-search launch shape overrides, e.g. ctas_per_sm=4,"
                     "bins_budget_words=10240 (cf_eval_tuning field names)")
     args = ap.parse_args()
     W.update(images=args.images, trees=args.trees, max_depth=args.max_depth,
-             predict_images=min(args.predict_images, args.images))
+             predict_images=min(args.predict_images, args.images), predict_trees=args.predict_trees)
     if args.impl == "reference":
         run_reference(args)
         return
@@ -312,27 +461,13 @@ def main():
             if ln.startswith("dram_bytes_per_feature_eval:"):
                 traffic = float(ln.split(":")[1]) * total_evals / max(1, eval_launches)
 
-    # prediction of 50 resident frames with the trained forest
-    n_pred = W["predict_images"]
+    # prediction: a forest of predict_trees trees trained with the same settings, 64 resident frames
     predict = None
-    if n_pred > 0:
-        forest = cf.Forest(ctx, trees)
-        probs = torch.empty((n_pred, W["classes"], W["height"], W["width"]), dtype=torch.float32, device=local)
-        lab = torch.empty((n_pred, W["height"], W["width"]), dtype=torch.uint8, device=local)
-        with torch.cuda.stream(stream):
-            forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
-            pstart, pend = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            pstart.record(stream)
-            reps = 3
-            for _ in range(reps):
-                forest.predict_dataset(ds, 0, n_pred, probs.data_ptr(), lab.data_ptr())
-            pend.record(stream)
-            torch.cuda.synchronize()
-        pred_ms = pstart.elapsed_time(pend) / reps
-        predict = {"images": n_pred, "mpx_per_s": n_pred * W["width"] * W["height"] / (pred_ms / 1e3) / 1e6,
-                   "ms_per_batch": pred_ms, "ms_per_frame": pred_ms / n_pred, "trees": W["trees"]}
-        forest.close()
+    if W["predict_images"] > 0:
+        ptrees = forest_trees(ds, labels, depth, cfg, W["predict_trees"])
+        predict = predict_section(ctx, stream, ds, ptrees, local, args.serve_seconds)
+        for t in ptrees:
+            t.close()
 
     # end to end through cf_forest_train with host buffers
     e2e = None
@@ -353,6 +488,30 @@ def main():
                "note": "cf_forest_train: upload, GPU integral images, host class-uniform sampling (one thread, "
                        "as the reference's reproducible mode), level-batched training, tree download"}
 
+    # the plain per-node form (reference-structured kernels: responses to HBM, one block per
+    # (threshold, feature), score kernel, host argmax, node by node) on this rank's first tree:
+    # same tree required, feature-evals/s compared
+    per_node = None
+    if not args.no_per_node:
+        t, s, prior, counter = per_tree[0]
+        res = {}
+        for name, mode in (("level_batched", cf.LEVEL_BATCHED), ("per_node", cf.PER_NODE)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            tree, _ = cf.train_tree(ds, s, W["classes"], cfg, tree_id=t, seed_counter=counter, mode=mode)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            res[name] = (tree.arrays(), e0.elapsed_time(e1), tree.train_stats()[0],
+                         [round(float(x[2]), 2) for x in tree.level_stats()])
+        (A, lb_ms, lb_ev, lb_lv), (B, pn_ms, pn_ev, pn_lv) = res["level_batched"], res["per_node"]
+        # leaves carry a NaN threshold, which must compare equal
+        identical = lb_ev == pn_ev and all(np.array_equal(A[k], B[k], equal_nan=A[k].dtype.kind == "f") for k in A)
+        per_node = {"value": pn_ev / (pn_ms / 1e3), "unit": "feature-evals/s", "ms_per_tree": pn_ms,
+                    "level_batched_value": lb_ev / (lb_ms / 1e3), "level_batched_ms_per_tree": lb_ms,
+                    "speedup": pn_ms / lb_ms, "trees_identical": bool(identical), "tree": int(t),
+                    "split_search_ms_per_level": {"per_node": pn_lv, "level_batched": lb_lv}}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _ = cpu_root_split_search(rgb, depth, labels, seconds=15.0)
@@ -372,6 +531,7 @@ def main():
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks.summary(),
                 "predict": predict,
+                "per_node": per_node,
                 "levels_tree0": [[n, s, round(ms, 3)] for n, s, ms in trees[0].level_stats()],
                 "feature_evals_per_step": total_evals / args.steps}
         print(json.dumps(line), flush=True)

@@ -484,6 +484,11 @@ class Forest:
         _check(lib().cf_predict_dataset(self.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
                                         _vp(labels_ptr)))
 
+    def predict_dataset_plain(self, ds, first, count, probs_ptr, labels_ptr):
+        """The plain per-image launch form (one launch per tree per image, synchronised)."""
+        _check(lib().cf_predict_dataset_plain(self.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
+                                              _vp(labels_ptr)))
+
     def predict(self, rgb, depth_mm, probabilities=True):
         rgb = np.ascontiguousarray(rgb, np.uint8)
         depth_mm = np.ascontiguousarray(depth_mm, np.uint16)
@@ -498,6 +503,42 @@ class Forest:
     def close(self):
         if self.handle:
             _check(lib().cf_forest_destroy(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PredictGraph:
+    """cf_predict_graph: a fixed batch of raw frames predicted by one CUDA graph replay. `rgb`,
+    `depth`, `labels` (and `probabilities`) are numpy views of the graph's pinned staging buffers."""
+
+    def __init__(self, forest, count, width, height, probabilities=False):
+        h = _vp()
+        _check(lib().cf_predict_graph_create(forest.handle, int(count), int(width), int(height), int(probabilities),
+                                             ctypes.byref(h)))
+        self.handle, self.forest = h, forest
+        rgb, dep, pr, lab = _vp(), _vp(), _vp(), _vp()
+        _check(lib().cf_predict_graph_buffers(h, ctypes.byref(rgb), ctypes.byref(dep), ctypes.byref(pr),
+                                              ctypes.byref(lab)))
+        n, C = int(count), forest.num_classes
+
+        def view(ptr, ctype, shape):
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctype)), shape=shape)
+        self.rgb = view(rgb, ctypes.c_uint8, (n, height, width, 3))
+        self.depth = view(dep, ctypes.c_uint16, (n, height, width))
+        self.labels = view(lab, ctypes.c_uint8, (n, height, width))
+        self.probabilities = view(pr, ctypes.c_float, (n, C, height, width)) if probabilities else None
+
+    def run(self):
+        _check(lib().cf_predict_graph_run(self.handle))
+
+    def close(self):
+        if self.handle:
+            _check(lib().cf_predict_graph_destroy(self.handle))
             self.handle = None
 
     def __del__(self):

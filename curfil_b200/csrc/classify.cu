@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 
+#include "eval_fast.cuh"
 #include "features.h"
 #include "forest.h"
 
@@ -61,14 +62,14 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
     if (p >= plane) return;
     const int y = static_cast<int>(p / fr.width);
     const int x = static_cast<int>(p - static_cast<long long>(y) * fr.width);
-    DsView ds;
-    ds.color = fr.color;
-    ds.depth = fr.depth;
-    ds.n = 1;
-    ds.width = fr.width;
-    ds.height = fr.height;
-    ds.plane = plane;
     const float depth = pixel_depth(fr.depth, fr.width, x, y);
+    EvalPixel px;
+    px.color = fr.color;
+    px.depth = fr.depth;
+    px.x = x;
+    px.y = y;
+    px.d = depth;
+    px.inv_d = depth > 0.0f ? __frcp_rn(depth) : 0.0f;
 
     float acc[CMAX];
 #pragma unroll
@@ -85,20 +86,12 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
             else nd = nodes[base + idx];
             meta = nd.meta;
             if (meta & 0x80000000u) break;
-            FeatParams fp;
-            fp.o1x = nd.o1x;
-            fp.o1y = nd.o1y;
-            fp.o2x = nd.o2x;
-            fp.o2y = nd.o2y;
-            fp.r1x = nd.r1x;
-            fp.r1y = nd.r1y;
-            fp.r2x = nd.r2x;
-            fp.r2y = nd.r2y;
-            fp.type = static_cast<uint8_t>((meta >> 26) & 1u);
-            fp.ch1 = static_cast<uint8_t>((meta >> 27) & 3u);
-            fp.ch2 = static_cast<uint8_t>((meta >> 29) & 3u);
-            const double r = feature_response(ds, 0, x, y, depth, fp, false);
-            idx = static_cast<int>(meta & 0x03FFFFFFu) + ((r <= static_cast<double>(nd.threshold)) ? 0 : 1);
+            // !(r <= threshold) for the exact double response (NaN right), decided on the fast
+            // path unless the threshold lies within its error bound
+            const EvalFeat ef = eval_feat_of(nd.o1x, nd.o1y, nd.o2x, nd.o2y, nd.r1x, nd.r1y, nd.r2x, nd.r2y,
+                                             (meta >> 26) & 1u, (meta >> 27) & 3u, (meta >> 29) & 3u);
+            idx = static_cast<int>(meta & 0x03FFFFFFu) +
+                  feature_bin(px, fr.width, fr.height, ef, false, ThresholdSide{nd.threshold});
         }
         const float* row = leaves + static_cast<long long>(meta & 0x7FFFFFFFu) * C;
 #pragma unroll
@@ -109,12 +102,18 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
 #pragma unroll
     for (int c = 0; c < CMAX; c++)
         if (c < C) sum = __dadd_rn(sum, static_cast<double>(acc[c]));
+    // RN(acc / sum) from the correctly rounded reciprocal with one correction step (Markstein,
+    // IBM J. Res. Dev. 34(1), 1990): q = RN(a y), r = a - q sum exactly by FMA, RN(q + r y)
+    const double inv = __drcp_rn(sum);
     float best = -1.0f;
     int label = 0;
 #pragma unroll
     for (int c = 0; c < CMAX; c++) {
         if (c < C) {
-            const float v = __double2float_rn(__ddiv_rn(static_cast<double>(acc[c]), sum));
+            const double a = static_cast<double>(acc[c]);
+            const double q = __dmul_rn(a, inv);
+            const double q1 = __fma_rn(__fma_rn(-q, sum, a), inv, q);
+            const float v = __double2float_rn(q1);
             if (fr.probs) fr.probs[c * plane + p] = v;
             if (v > best) {
                 best = v;
@@ -125,12 +124,84 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
     if (fr.labels) fr.labels[p] = static_cast<uint8_t>(label);
 }
 
+// ---- the plain per-image launch form (classifyImage, random_tree_image_gpu.cu:1414-1453): per image
+// and tree one launch that walks that tree with the exact double response and adds the leaf
+// histogram into probabilities [C][H][W] in global memory, then a normalisation launch and an
+// argmax launch, each followed by a stream synchronisation as the reference's mutex-guarded loop.
+__global__ void plain_classify_tree_kernel(const PackedNode* __restrict__ nodes, int base,
+                                           const float* __restrict__ leaves, int C, FrameDesc fr) {
+    const long long plane = static_cast<long long>(fr.width) * fr.height;
+    const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= plane) return;
+    const int y = static_cast<int>(p / fr.width);
+    const int x = static_cast<int>(p - static_cast<long long>(y) * fr.width);
+    DsView ds;
+    ds.color = fr.color;
+    ds.depth = fr.depth;
+    ds.n = 1;
+    ds.width = fr.width;
+    ds.height = fr.height;
+    ds.plane = plane;
+    const float depth = pixel_depth(fr.depth, fr.width, x, y);
+    int idx = 0;
+    uint32_t meta;
+    for (;;) {
+        const PackedNode nd = nodes[base + idx];
+        meta = nd.meta;
+        if (meta & 0x80000000u) break;
+        FeatParams fp;
+        fp.o1x = nd.o1x;
+        fp.o1y = nd.o1y;
+        fp.o2x = nd.o2x;
+        fp.o2y = nd.o2y;
+        fp.r1x = nd.r1x;
+        fp.r1y = nd.r1y;
+        fp.r2x = nd.r2x;
+        fp.r2y = nd.r2y;
+        fp.type = static_cast<uint8_t>((meta >> 26) & 1u);
+        fp.ch1 = static_cast<uint8_t>((meta >> 27) & 3u);
+        fp.ch2 = static_cast<uint8_t>((meta >> 29) & 3u);
+        fp.pad = 0;
+        const double r = feature_response(ds, 0, x, y, depth, fp, false);
+        idx = static_cast<int>(meta & 0x03FFFFFFu) + ((r <= static_cast<double>(nd.threshold)) ? 0 : 1);
+    }
+    const float* row = leaves + static_cast<long long>(meta & 0x7FFFFFFFu) * C;
+    for (int c = 0; c < C; c++) fr.probs[c * plane + p] = __fadd_rn(fr.probs[c * plane + p], __ldg(row + c));
+}
+
+__global__ void plain_normalize_kernel(float* __restrict__ probs, int C, long long plane) {
+    const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= plane) return;
+    double sum = 0.0;
+    for (int c = 0; c < C; c++) sum = __dadd_rn(sum, static_cast<double>(probs[c * plane + p]));
+    for (int c = 0; c < C; c++)
+        probs[c * plane + p] = __double2float_rn(__ddiv_rn(static_cast<double>(probs[c * plane + p]), sum));
+}
+
+__global__ void plain_argmax_kernel(const float* __restrict__ probs, int C, long long plane, uint8_t* __restrict__ labels) {
+    const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= plane) return;
+    float best = -1.0f;
+    int label = 0;
+    for (int c = 0; c < C; c++) {
+        const float v = probs[c * plane + p];
+        if (v > best) {
+            best = v;
+            label = c;
+        }
+    }
+    labels[p] = static_cast<uint8_t>(label);
+}
+
 template <int CMAX>
 void launch_classify(cf_context* ctx, cudaStream_t stream, const cf_forest* f, const FrameDesc* frames, int num_frames,
                      int blocks) {
     const size_t smem = sizeof(PackedNode) * f->num_trees * f->cache_per_tree;
-    CF_CUDA_CHECK(cudaFuncSetAttribute(classify_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(std::max<size_t>(smem, 1))));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CF_CUDA_CHECK(cudaStreamIsCapturing(stream, &cs));
+    if (cs == cudaStreamCaptureStatusNone)   // set before capture (an uncaptured pass runs first)
+        CF_CUDA_CHECK(cudaFuncSetAttribute(classify_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(std::max<size_t>(smem, 1))));
     launch_on(ctx, stream, "classify", dim3(blocks), dim3(kClassifyThreads), smem, classify_kernel<CMAX>, f->nodes.get(),
            f->d_tree_base.get(), f->num_trees, f->cache_per_tree, f->leaves.get(), f->C, frames, num_frames);
 }
@@ -353,6 +424,195 @@ cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, c
         if (labels)
             CF_CUDA_CHECK(cudaMemcpyAsync(labels, forest->labels.get(), plane * count, cudaMemcpyDeviceToHost, ctx->stream));
         CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_predict_dataset_plain(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
+                                   uint8_t* labels) {
+    return guard([&] {
+        CF_REQUIRE(forest && ds, "cf_predict_dataset_plain: NULL argument");
+        CF_REQUIRE(first >= 0 && count >= 1 && first + count <= ds->n, "cf_predict_dataset_plain: image range");
+        CF_REQUIRE(ds->ctx == forest->ctx, "cf_predict_dataset_plain: dataset and forest belong to different contexts");
+        cf_context* ctx = forest->ctx;
+        make_current(ctx);
+        const int C = forest->C;
+        const long long plane = static_cast<long long>(ds->width) * ds->height;
+        const unsigned blocks = static_cast<unsigned>((plane + 255) / 256);
+        if (!probabilities) forest->probs.reserve(static_cast<size_t>(plane) * C);
+        if (!labels) forest->labels.reserve(static_cast<size_t>(plane));
+        cudaStream_t st = ctx->stream;
+        for (int i = 0; i < count; i++) {
+            FrameDesc fr;
+            fr.color = ds->color.get() + (first + i) * plane * 3;
+            fr.depth = ds->depth.get() + (first + i) * plane;
+            fr.probs = probabilities ? probabilities + static_cast<long long>(i) * C * plane : forest->probs.get();
+            fr.labels = labels ? labels + static_cast<long long>(i) * plane : forest->labels.get();
+            fr.width = ds->width;
+            fr.height = ds->height;
+            fr.first_block = 0;
+            fr.pad = 0;
+            CF_CUDA_CHECK(cudaMemsetAsync(fr.probs, 0, sizeof(float) * C * plane, st));
+            for (int t = 0; t < forest->num_trees; t++) {
+                launch(ctx, "plain_classify", dim3(blocks), dim3(256), 0, plain_classify_tree_kernel, forest->nodes.get(),
+                       forest->tree_base[t], forest->leaves.get(), C, fr);
+                CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            }
+            launch(ctx, "plain_normalize", dim3(blocks), dim3(256), 0, plain_normalize_kernel, fr.probs, C, plane);
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            launch(ctx, "plain_argmax", dim3(blocks), dim3(256), 0, plain_argmax_kernel, fr.probs, C, plane, fr.labels);
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+        }
+    });
+}
+
+}  // extern "C"
+
+// ---- batch prediction captured as a CUDA graph ----------------------------------------------------
+struct cf_predict_graph {
+    cf_forest* forest = nullptr;
+    int count = 0, width = 0, height = 0;
+    bool with_probs = false;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;   // kernel nodes per replay
+    cf::PinnedBuffer h_rgb, h_depth, h_probs, h_labels;
+    cf::DevArray<uint8_t> rgb;
+    cf::DevArray<uint16_t> depth_mm;
+    cf::DevArray<float> color;
+    cf::DevArray<int2> dint;
+    cf::DevArray<float> probs;
+    cf::DevArray<uint8_t> labels;
+    cf::DevArray<cf::FrameDesc> frames;
+
+    ~cf_predict_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// One batch: pinned inputs -> device, integral images, classification, results -> pinned outputs.
+void enqueue_graph_batch(cf_predict_graph* g, int blocks) {
+    cf_context* ctx = g->forest->ctx;
+    const size_t plane = static_cast<size_t>(g->width) * g->height;
+    const size_t n = static_cast<size_t>(g->count);
+    CF_CUDA_CHECK(cudaMemcpyAsync(g->rgb.get(), g->h_rgb.get(), plane * 3 * n, cudaMemcpyHostToDevice, g->stream));
+    CF_CUDA_CHECK(cudaMemcpyAsync(g->depth_mm.get(), g->h_depth.get(), plane * 2 * n, cudaMemcpyHostToDevice, g->stream));
+    integrate_frames(ctx, g->rgb.get(), g->depth_mm.get(), g->count, g->width, g->height, g->color.get(), g->dint.get(),
+                     g->stream);
+    classify_frames(ctx, g->forest, g->frames.get(), g->count, blocks, g->stream);
+    CF_CUDA_CHECK(cudaMemcpyAsync(g->h_labels.get(), g->labels.get(), plane * n, cudaMemcpyDeviceToHost, g->stream));
+    if (g->with_probs)
+        CF_CUDA_CHECK(cudaMemcpyAsync(g->h_probs.get(), g->probs.get(), sizeof(float) * plane * g->forest->C * n,
+                                      cudaMemcpyDeviceToHost, g->stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+cf_status cf_predict_graph_create(cf_forest* forest, int count, int width, int height, int with_probabilities,
+                                  cf_predict_graph** out) {
+    return guard([&] {
+        CF_REQUIRE(forest && out, "cf_predict_graph_create: NULL argument");
+        CF_REQUIRE(count >= 1 && width >= 1 && height >= 1, "cf_predict_graph_create: empty batch");
+        cf_context* ctx = forest->ctx;
+        make_current(ctx);
+        auto* g = new cf_predict_graph();
+        std::unique_ptr<cf_predict_graph> own(g);
+        g->forest = forest;
+        g->count = count;
+        g->width = width;
+        g->height = height;
+        g->with_probs = with_probabilities != 0;
+        const size_t plane = static_cast<size_t>(width) * height;
+        const size_t n = static_cast<size_t>(count);
+        const int C = forest->C;
+        g->h_rgb.reserve(plane * 3 * n);
+        g->h_depth.reserve(plane * 2 * n);
+        g->h_labels.reserve(plane * n);
+        if (g->with_probs) g->h_probs.reserve(sizeof(float) * plane * C * n);
+        std::memset(g->h_rgb.get(), 0, plane * 3 * n);
+        std::memset(g->h_depth.get(), 0, plane * 2 * n);
+        g->rgb.reserve(plane * 3 * n);
+        g->depth_mm.reserve(plane * n);
+        g->color.reserve(plane * 3 * n);
+        g->dint.reserve(plane * n);
+        g->labels.reserve(plane * n);
+        if (g->with_probs) g->probs.reserve(plane * C * n);
+        std::vector<FrameDesc> frames(n);
+        int blocks = 0;
+        for (size_t i = 0; i < n; i++) {
+            FrameDesc& fr = frames[i];
+            fr.color = g->color.get() + plane * 3 * i;
+            fr.depth = g->dint.get() + plane * i;
+            fr.probs = g->with_probs ? g->probs.get() + plane * C * i : nullptr;
+            fr.labels = g->labels.get() + plane * i;
+            fr.width = width;
+            fr.height = height;
+            fr.first_block = blocks;
+            fr.pad = 0;
+            blocks += classify_blocks_for(width, height);
+        }
+        g->frames.reserve(n);
+        CF_CUDA_CHECK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        CF_CUDA_CHECK(cudaMemcpyAsync(g->frames.get(), frames.data(), sizeof(FrameDesc) * n, cudaMemcpyHostToDevice,
+                                      g->stream));
+        // one uncaptured pass sets the kernels' attributes and checks the pipeline, then capture
+        enqueue_graph_batch(g, blocks);
+        CF_CUDA_CHECK(cudaStreamSynchronize(g->stream));
+        const int64_t before = ctx->launches.load();
+        CF_CUDA_CHECK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue_graph_batch(g, blocks);
+        } catch (...) {
+            cudaGraph_t broken = nullptr;
+            cudaStreamEndCapture(g->stream, &broken);
+            if (broken) cudaGraphDestroy(broken);
+            throw;
+        }
+        CF_CUDA_CHECK(cudaStreamEndCapture(g->stream, &g->graph));
+        g->kernels = ctx->launches.load() - before;
+        ctx->launches -= g->kernels;   // counted when the graph runs
+        CF_CUDA_CHECK(cudaGraphInstantiate(&g->exec, g->graph, 0));
+        context_retain(ctx);
+        *out = own.release();
+    });
+}
+
+cf_status cf_predict_graph_buffers(cf_predict_graph* g, uint8_t** rgb, uint16_t** depth_mm, float** probabilities,
+                                   uint8_t** labels) {
+    return guard([&] {
+        CF_REQUIRE(g, "cf_predict_graph_buffers: graph is NULL");
+        if (rgb) *rgb = static_cast<uint8_t*>(g->h_rgb.get());
+        if (depth_mm) *depth_mm = static_cast<uint16_t*>(g->h_depth.get());
+        if (probabilities) *probabilities = g->with_probs ? static_cast<float*>(g->h_probs.get()) : nullptr;
+        if (labels) *labels = static_cast<uint8_t*>(g->h_labels.get());
+    });
+}
+
+cf_status cf_predict_graph_run(cf_predict_graph* g) {
+    return guard([&] {
+        CF_REQUIRE(g, "cf_predict_graph_run: graph is NULL");
+        cf_context* ctx = g->forest->ctx;
+        make_current(ctx);
+        CF_CUDA_CHECK(cudaGraphLaunch(g->exec, g->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(g->stream));
+        ctx->launches += g->kernels;
+    });
+}
+
+cf_status cf_predict_graph_destroy(cf_predict_graph* g) {
+    return guard([&] {
+        if (!g) return;
+        cf_context* ctx = g->forest->ctx;
+        cudaSetDevice(ctx->device);
+        if (g->stream) cudaStreamSynchronize(g->stream);
+        delete g;
+        context_release(ctx);
     });
 }
 

@@ -33,6 +33,10 @@ void context_release(cf_context* ctx) {
 LaunchScope::LaunchScope(cf_context* ctx, cudaStream_t stream, const char* name)
     : ctx_(ctx), stream_(stream), name_(name) {
     if (ctx_->timing) {
+        // launches recorded into a CUDA graph are not timed one by one
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CF_CUDA_CHECK(cudaStreamIsCapturing(stream_, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return;
         std::lock_guard<std::mutex> lock(ctx_->mu);
         start_ = ctx_->take_event();
         CF_CUDA_CHECK(cudaEventRecord(start_, stream_));

@@ -77,7 +77,8 @@ __device__ __forceinline__ EvalFeat make_eval_feat(const FeatParams& f) {
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         e.v[i] = v[i];
-        e.av[i] = static_cast<float>(v[i] < 0 ? -v[i] : v[i]);
+        // |v| <= 128 converts exactly through the float bit pattern of 2^23 + |v|
+        e.av[i] = __fsub_rn(__int_as_float(0x4B000000 | (v[i] < 0 ? -v[i] : v[i])), 8388608.0f);
     }
     e.type = f.type;
     e.ch1 = f.ch1;
@@ -122,17 +123,43 @@ __device__ __forceinline__ int exact_bin(double r, const float* sorted, int T) {
     return count_below<kPad32>(sorted, T, __double2float_ru(r));
 }
 
-// exact depth response ((s1/1000)/n1 - (s2/1000)/n2 in double, random_tree_image.h:313-315) binned
-template <bool kPad32>
-static __device__ __noinline__ int exact_depth_bin(int s1, int nv1, int s2, int nv2, const float* sorted, int T) {
+// exact depth response ((s1/1000)/n1 - (s2/1000)/n2 in double, random_tree_image.h:313-315)
+static __device__ __noinline__ double exact_depth_response(int s1, int nv1, int s2, int nv2) {
     const double A = __ddiv_rn(__ddiv_rn(static_cast<double>(s1), 1000.0), static_cast<double>(nv1));
     const double B = __ddiv_rn(__ddiv_rn(static_cast<double>(s2), 1000.0), static_cast<double>(nv2));
-    return exact_bin<kPad32>(__dsub_rn(A, B), sorted, T);
+    return __dsub_rn(A, B);
 }
 
+// Binning policies of feature_bin.
+// SortedBins: the number of a feature's sorted thresholds t with !(r <= t) (0..T; NaN -> T).
 template <bool kPad32>
+struct SortedBins {
+    const float* sorted;
+    int T;
+    __device__ __forceinline__ int nan() const { return T; }
+    // bin of every r in [r0 - delta, r0 + delta] if it is the same for all of them
+    __device__ __forceinline__ bool fast(float r0, float delta, int& k) const {
+        k = count_below<kPad32>(sorted, T, r0 - delta);
+        return (!kPad32 && k == T) || sorted[k] > r0 + delta;
+    }
+    __device__ __forceinline__ int exact(double r) const { return exact_bin<kPad32>(r, sorted, T); }
+};
+
+// ThresholdSide: 1 when the sample goes right of one split, !(r <= threshold) (NaN goes right).
+struct ThresholdSide {
+    float thr;
+    __device__ __forceinline__ int nan() const { return 1; }
+    __device__ __forceinline__ bool fast(float r0, float delta, int& k) const {
+        k = r0 - delta > thr ? 1 : 0;
+        return r0 - delta > thr || r0 + delta < thr;
+    }
+    __device__ __forceinline__ int exact(double r) const { return r <= static_cast<double>(thr) ? 0 : 1; }
+};
+
+template <typename Bins>
 __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, const EvalFeat& f, bool flip,
-                                           const float* sorted, int T) {
+                                           const Bins& bins) {
+    const int T = bins.nan();
     if (!(p.d > 0.0f)) return T;
     const int o1x = flip ? -f.v[0] : f.v[0];
     const int o2x = flip ? -f.v[2] : f.v[2];
@@ -169,9 +196,9 @@ __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, con
         const float b = __fdividef(static_cast<float>(s2), n2f) * 0.001f;
         const float r = a - b;
         const float delta = 2e-6f * (fabsf(a) + fabsf(b)) + 1e-30f;
-        const int k = count_below<kPad32>(sorted, T, r - delta);
-        if ((!kPad32 && k == T) || sorted[k] > r + delta) return k;
-        return exact_depth_bin<kPad32>(s1, nv1, s2, nv2, sorted, T);
+        int k;
+        if (bins.fast(r, delta, k)) return k;
+        return bins.exact(exact_depth_response(s1, nv1, s2, nv2));
     }
     const float* P1 = p.color + static_cast<long long>(f.ch1) * W * H;
     const float* P2 = p.color + static_cast<long long>(f.ch2) * W * H;
@@ -184,7 +211,26 @@ __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, con
                                __dsub_rn(static_cast<double>(c_ul), static_cast<double>(c_ll)));
     const double B = __dadd_rn(__dsub_rn(static_cast<double>(d_lr), static_cast<double>(d_ur)),
                                __dsub_rn(static_cast<double>(d_ul), static_cast<double>(d_ll)));
-    return exact_bin<kPad32>(__dsub_rn(A, B), sorted, T);
+    return bins.exact(__dsub_rn(A, B));
+}
+
+// Feature parameters of a packed split node, prepared for feature_bin.
+__device__ __forceinline__ EvalFeat eval_feat_of(int8_t o1x, int8_t o1y, int8_t o2x, int8_t o2y, int8_t r1x,
+                                                 int8_t r1y, int8_t r2x, int8_t r2y, int type, int ch1, int ch2) {
+    FeatParams fp;
+    fp.o1x = o1x;
+    fp.o1y = o1y;
+    fp.o2x = o2x;
+    fp.o2y = o2y;
+    fp.r1x = r1x;
+    fp.r1y = r1y;
+    fp.r2x = r2x;
+    fp.r2y = r2y;
+    fp.type = static_cast<uint8_t>(type);
+    fp.ch1 = static_cast<uint8_t>(ch1);
+    fp.ch2 = static_cast<uint8_t>(ch2);
+    fp.pad = 0;
+    return make_eval_feat(fp);
 }
 
 }  // namespace cf

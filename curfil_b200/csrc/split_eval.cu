@@ -30,22 +30,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ int bin_of(double r, const float* sorted, int T) {
-    if (isnan(r)) return T;
-    const float ru = __double2float_ru(r);
-    int lo = 0, n = T;
-    while (n > 0) {
-        const int half = n >> 1;
-        if (sorted[lo + half] < ru) {
-            lo += half + 1;
-            n -= half + 1;
-        } else {
-            n = half;
-        }
-    }
-    return lo;
-}
-
 template <bool kAgg>
 __device__ __forceinline__ void bin_increment(uint32_t* bins, int key) {
     if (kAgg) {
@@ -244,29 +228,29 @@ level_eval_kernel(EvalArgs a) {
                 for (; f + 1 < nf; f += 2) {
                     const EvalFeat& fa = s_params[f];
                     const EvalFeat& fb = s_params[f + 1];
-                    const float* sa = s_thr + f * TP;
-                    const float* sb = sa + TP;
+                    const SortedBins<kPad32> sa{s_thr + f * TP, T};
+                    const SortedBins<kPad32> sb{s_thr + (f + 1) * TP, T};
                     const int row_a = (f * cp + lid) * T1;
                     const int row_b = row_a + cp * T1;
-                    const int ka = row_a + feature_bin<kPad32>(px, W, H, fa, flip == 1, sa, T);
-                    const int kb = row_b + feature_bin<kPad32>(px, W, H, fb, flip == 1, sb, T);
+                    const int ka = row_a + feature_bin(px, W, H, fa, flip == 1, sa);
+                    const int kb = row_b + feature_bin(px, W, H, fb, flip == 1, sb);
                     bin_increment<kAgg>(s_bins, ka);
                     bin_increment<kAgg>(s_bins, kb);
                     if (any_both) {
-                        const int ka2 = flip == 2 ? row_a + feature_bin<kPad32>(px, W, H, fa, true, sa, T) : -1;
-                        const int kb2 = flip == 2 ? row_b + feature_bin<kPad32>(px, W, H, fb, true, sb, T) : -1;
+                        const int ka2 = flip == 2 ? row_a + feature_bin(px, W, H, fa, true, sa) : -1;
+                        const int kb2 = flip == 2 ? row_b + feature_bin(px, W, H, fb, true, sb) : -1;
                         bin_increment<kAgg>(s_bins, ka2);
                         bin_increment<kAgg>(s_bins, kb2);
                     }
                 }
                 if (f < nf) {
                     const EvalFeat& fp = s_params[f];
-                    const float* sorted = s_thr + f * TP;
+                    const SortedBins<kPad32> sorted{s_thr + f * TP, T};
                     const int row = (f * cp + lid) * T1;
-                    const int key1 = row + feature_bin<kPad32>(px, W, H, fp, flip == 1, sorted, T);
+                    const int key1 = row + feature_bin(px, W, H, fp, flip == 1, sorted);
                     bin_increment<kAgg>(s_bins, key1);
                     if (any_both) {
-                        const int key2 = flip == 2 ? row + feature_bin<kPad32>(px, W, H, fp, true, sorted, T) : -1;
+                        const int key2 = flip == 2 ? row + feature_bin(px, W, H, fp, true, sorted) : -1;
                         bin_increment<kAgg>(s_bins, key2);
                     }
                 }
@@ -288,10 +272,10 @@ level_eval_kernel(EvalArgs a) {
                         const Sample smp = tail[s];
                         const EvalPixel px = make_eval_pixel(a.ds, smp);
                         const EvalFeat& fp = s_params[f];
-                        const float* sorted = s_thr + f * TP;
+                        const SortedBins<kPad32> sorted{s_thr + f * TP, T};
                         const int row = (f * cp + s_lid[smp.label]) * T1;
-                        key1 = row + feature_bin<kPad32>(px, W, H, fp, smp.flip == 1, sorted, T);
-                        if (smp.flip == 2) key2 = row + feature_bin<kPad32>(px, W, H, fp, true, sorted, T);
+                        key1 = row + feature_bin(px, W, H, fp, smp.flip == 1, sorted);
+                        if (smp.flip == 2) key2 = row + feature_bin(px, W, H, fp, true, sorted);
                     }
                     bin_increment<kAgg>(s_bins, key1);
                     if (__any_sync(kFull, key2 >= 0)) bin_increment<kAgg>(s_bins, key2);
@@ -536,7 +520,6 @@ __global__ void score_bounds_kernel(const uint32_t* __restrict__ counters, const
 __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const uint32_t* __restrict__ hist, int C, int F,
                                    int T, double* __restrict__ scores) {
     __shared__ double s_hc;
-    __shared__ double s_total;
     if (threadIdx.x == 0) {
         double total = 0, hc = 0;
         for (int c = 0; c < C; c++) total += static_cast<double>(hist[c]);
@@ -544,7 +527,6 @@ __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const 
             if (hist[c] > 0) hc = __dadd_rn(hc, entropy_of(static_cast<double>(hist[c])));
         hc = __dsub_rn(hc, entropy_of(total));
         s_hc = __ddiv_rn(hc, total);
-        s_total = total;
     }
     __syncthreads();
     const int feature = blockIdx.x * blockDim.x + threadIdx.x;

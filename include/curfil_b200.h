@@ -265,6 +265,26 @@ cf_status cf_predict_dataset(cf_forest* forest, cf_dataset* ds, int first, int c
 /* Same from raw host frames, results to host buffers (either may be NULL). */
 cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, const uint8_t* rgb,
                           const uint16_t* depth_mm, float* probabilities, uint8_t* labels);
+/* The plain per-image launch form of classifyImage (random_tree_image_gpu.cu:1414-1453): per image,
+ * one launch per tree accumulating into probabilities, then normalisation and argmax launches, each
+ * followed by a stream synchronisation. Same results as cf_predict_dataset; kept as the baseline the
+ * batched form is measured against. DEVICE pointers, either may be NULL. */
+cf_status cf_predict_dataset_plain(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
+                                   uint8_t* labels);
+
+/* A fixed batch of `count` raw frames (width x height) captured once as a CUDA graph: host-to-device
+ * copy from pinned staging buffers, integral images, classification, results back to pinned buffers.
+ * Project extension with no reference counterpart. Fill the buffers returned by
+ * cf_predict_graph_buffers (rgb uint8 [count][H][W][3], depth uint16 [count][H][W]), call run, read
+ * labels uint8 [count][H][W] and, when requested at creation, probabilities float [count][C][H][W].
+ * Destroy the graph before its forest. */
+typedef struct cf_predict_graph cf_predict_graph;
+cf_status cf_predict_graph_create(cf_forest* forest, int count, int width, int height, int with_probabilities,
+                                  cf_predict_graph** out);
+cf_status cf_predict_graph_buffers(cf_predict_graph* graph, uint8_t** rgb, uint16_t** depth_mm, float** probabilities,
+                                   uint8_t** labels);
+cf_status cf_predict_graph_run(cf_predict_graph* graph);
+cf_status cf_predict_graph_destroy(cf_predict_graph* graph);
 
 /* ---------------------------------------------------------------------------------------------
  * Serving: continuous batching of mixed-resolution frames on a resident forest

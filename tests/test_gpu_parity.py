@@ -341,6 +341,42 @@ def test_predict_dataset_equals_host_path(ctx, scene, forest_and_oracle):
     np.testing.assert_array_equal(labels_d.cpu().numpy(), labels_h)
 
 
+def test_predict_batched_equals_plain_per_image(ctx, scene, forest_and_oracle):
+    """The batched kernel (fast-path responses with exact fallback, reciprocal-corrected division) and
+    the reference-structured plain form (exact double responses, one launch per tree and image, plain
+    division) agree bit for bit. Thresholds are responses of training pixels, so the training frames
+    hit responses equal to thresholds and exercise the fallback."""
+    import torch
+    forest, _, _ = forest_and_oracle
+    n, h, w = scene["depth"].shape
+    pa = torch.empty((n, 40, h, w), dtype=torch.float32, device="cuda:0")
+    la = torch.empty((n, h, w), dtype=torch.uint8, device="cuda:0")
+    pb = torch.empty_like(pa)
+    lb = torch.empty_like(la)
+    ctx.synchronize()
+    forest.predict_dataset(scene["ds"], 0, n, pa.data_ptr(), la.data_ptr())
+    forest.predict_dataset_plain(scene["ds"], 0, n, pb.data_ptr(), lb.data_ptr())
+    ctx.synchronize()
+    np.testing.assert_array_equal(pa.cpu().numpy().view(np.uint32), pb.cpu().numpy().view(np.uint32))
+    np.testing.assert_array_equal(la.cpu().numpy(), lb.cpu().numpy())
+
+
+def test_predict_graph_equals_host_path(ctx, forest_and_oracle):
+    forest, _, _ = forest_and_oracle
+    g = cf.PredictGraph(forest, 3, 96, 72, probabilities=True)
+    try:
+        for seed in (123, 124):
+            rgb, depth, _ = H.frames(seed=seed, n=3, w=96, h=72, cells=12, classes=40)
+            g.rgb[...] = rgb
+            g.depth[...] = depth
+            g.run()
+            probs, labels = forest.predict(rgb, depth)
+            np.testing.assert_array_equal(g.labels, labels)
+            np.testing.assert_array_equal(g.probabilities, probs)
+    finally:
+        g.close()
+
+
 def test_forest_train_end_to_end_matches_oracle(ctx):
     """RandomForestImage::train on raw frames (sampling on the host) vs oracle sampling + training."""
     rgb, depth, labels = H.frames(seed=5, n=3, w=80, h=60, cells=10, classes=6)
