@@ -273,6 +273,18 @@ def predict_section(ctx, stream, ds, trees, local, serve_seconds):
     out["graph_e2e"] = {"mpx_per_s": px / gs / 1e6, "ms_per_batch": gs * 1e3,
                         "h2d_bytes_per_batch": int(rgb.nbytes + depth.nbytes), "d2h_bytes_per_batch": int(px),
                         "note": "pinned host RGB-D -> H2D -> integral images -> classify -> labels D2H, one graph"}
+    # the plain per-image form from the same host frames, as RandomForestImage::predict runs on the
+    # GPU: upload, one launch + sync per tree, normalise, argmax, probabilities and labels copied back
+    sub = min(n, 16)
+    forest.predict_plain(rgb[:1], depth[:1], probabilities=False)
+    t0 = time.perf_counter()
+    _, lp = forest.predict_plain(rgb[:sub], depth[:sub], probabilities=False)
+    ps = time.perf_counter() - t0
+    spx = sub * H * Wd
+    out["plain_per_image_host"] = {"mpx_per_s": spx / ps / 1e6, "frames": sub, "ms_per_frame": ps * 1e3 / sub,
+                                   "d2h_bytes_per_frame": H * Wd * (4 * C + 1)}
+    out["e2e_speedup_vs_plain"] = (px / gs) / (spx / ps)
+    out["e2e_labels_identical"] = bool(np.array_equal(lp, g.labels[:sub]))
     g.close()
     if serve_seconds > 0:
         out["serving"] = serve(forest, serve_seconds)

@@ -489,6 +489,18 @@ class Forest:
         _check(lib().cf_predict_dataset_plain(self.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
                                               _vp(labels_ptr)))
 
+    def predict_plain(self, rgb, depth_mm, probabilities=True):
+        """RandomForestImage::predict's GPU flow image by image (the plain per-image launch form)."""
+        rgb = np.ascontiguousarray(rgb, np.uint8)
+        depth_mm = np.ascontiguousarray(depth_mm, np.uint16)
+        if depth_mm.ndim == 2:
+            rgb, depth_mm = rgb[None], depth_mm[None]
+        n, h, w = depth_mm.shape
+        probs = np.empty((n, self.num_classes, h, w), np.float32) if probabilities else None
+        labels = np.empty((n, h, w), np.uint8)
+        _check(lib().cf_predict_host_plain(self.handle, n, w, h, _p(rgb), _p(depth_mm), _p(probs), _p(labels)))
+        return probs, labels
+
     def predict(self, rgb, depth_mm, probabilities=True):
         rgb = np.ascontiguousarray(rgb, np.uint8)
         depth_mm = np.ascontiguousarray(depth_mm, np.uint16)

@@ -23,6 +23,8 @@ namespace {
 
 constexpr int kClassifyThreads = 256;
 constexpr int kSmemNodesBudget = 2048;  // 32 KB of cached nodes per CTA
+constexpr int kTreeChunk = 32;          // trees walked before their leaves are summed
+constexpr int kTileW = 32, kTileH = 8;  // pixels of one classify CTA (8 warps of 8x4)
 
 __device__ __forceinline__ float pixel_depth(const int2* D, int W, int x, int y) {
     const int2 c = __ldg(D + static_cast<long long>(y) * W + x);
@@ -37,12 +39,18 @@ __device__ __forceinline__ float pixel_depth(const int2* D, int W, int x, int y)
     return __fdiv_rn(static_cast<float>(mm), 1000.0f);
 }
 
+// A CTA covers 32x8 pixels, each warp an 8x4 tile, so the lanes of a warp are close in both
+// directions and mostly walk the same nodes. Each lane moves on to its next tree as soon as it
+// reaches a leaf (lanes do not wait at tree boundaries for the deepest path of the warp) and only
+// records the leaf ([tree][threads] after the node cache); the histograms are summed afterwards,
+// all lanes together, in tree order.
 template <int CMAX>
-__global__ void __launch_bounds__(kClassifyThreads)
+__global__ void __launch_bounds__(kClassifyThreads, CMAX <= 64 ? 4 : 1)
 classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tree_base, int num_trees, int cache,
                 const float* __restrict__ leaves, int C, const FrameDesc* __restrict__ frames, int num_frames) {
     extern __shared__ __align__(16) unsigned char smem[];
     PackedNode* s_nodes = reinterpret_cast<PackedNode*>(smem);
+    uint32_t* my_leaf = reinterpret_cast<uint32_t*>(smem + sizeof(PackedNode) * num_trees * cache) + threadIdx.x;
     // which frame does this CTA serve
     int lo = 0, hi = num_frames - 1;
     while (lo < hi) {
@@ -58,10 +66,13 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
     }
     __syncthreads();
     const long long plane = static_cast<long long>(fr.width) * fr.height;
-    const long long p = static_cast<long long>(blockIdx.x - fr.first_block) * blockDim.x + threadIdx.x;
-    if (p >= plane) return;
-    const int y = static_cast<int>(p / fr.width);
-    const int x = static_cast<int>(p - static_cast<long long>(y) * fr.width);
+    const int b = static_cast<int>(blockIdx.x) - fr.first_block;
+    const int bw = (fr.width + kTileW - 1) / kTileW;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = (b % bw) * kTileW + (warp & 3) * 8 + (lane & 7);
+    const int y = (b / bw) * kTileH + (warp >> 2) * 4 + (lane >> 3);
+    if (x >= fr.width || y >= fr.height) return;
+    const long long p = static_cast<long long>(y) * fr.width + x;
     const float depth = pixel_depth(fr.depth, fr.width, x, y);
     EvalPixel px;
     px.color = fr.color;
@@ -72,20 +83,23 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
     px.inv_d = depth > 0.0f ? __frcp_rn(depth) : 0.0f;
 
     float acc[CMAX];
-#pragma unroll
-    for (int c = 0; c < CMAX; c++) acc[c] = 0.0f;
-    for (int t = 0; t < num_trees; t++) {
-        const int base = tree_base[t];
-        const int nt = tree_base[t + 1] - base;
-        const int cached = min(cache, nt);
-        int idx = 0;
-        uint32_t meta;
-        for (;;) {
-            PackedNode nd;
-            if (idx < cached) nd = s_nodes[t * cache + idx];
-            else nd = nodes[base + idx];
-            meta = nd.meta;
-            if (meta & 0x80000000u) break;
+    for (int t0 = 0; t0 < num_trees; t0 += kTreeChunk) {
+        const int t1 = min(num_trees, t0 + kTreeChunk);
+        int t = t0, idx = 0;
+        int base = tree_base[t];
+        int cached = min(cache, tree_base[t + 1] - base);
+        while (t < t1) {
+            const PackedNode nd = idx < cached ? s_nodes[t * cache + idx] : nodes[base + idx];
+            const uint32_t meta = nd.meta;
+            if (meta & 0x80000000u) {
+                my_leaf[(t - t0) * kClassifyThreads] = meta & 0x7FFFFFFFu;
+                if (++t < t1) {
+                    base = tree_base[t];
+                    cached = min(cache, tree_base[t + 1] - base);
+                }
+                idx = 0;
+                continue;
+            }
             // !(r <= threshold) for the exact double response (NaN right), decided on the fast
             // path unless the threshold lies within its error bound
             const EvalFeat ef = eval_feat_of(nd.o1x, nd.o1y, nd.o2x, nd.o2y, nd.r1x, nd.r1y, nd.r2x, nd.r2y,
@@ -93,15 +107,19 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
             idx = static_cast<int>(meta & 0x03FFFFFFu) +
                   feature_bin(px, fr.width, fr.height, ef, false, ThresholdSide{nd.threshold});
         }
-        const float* row = leaves + static_cast<long long>(meta & 0x7FFFFFFFu) * C;
+        // the leaves' normalised histograms, summed in tree order as the reference sums them
+        for (int tt = t0; tt < t1; tt++) {
+            const float* row = leaves + static_cast<long long>(my_leaf[(tt - t0) * kClassifyThreads]) * C;
 #pragma unroll
-        for (int c = 0; c < CMAX; c++)
-            if (c < C) acc[c] = __fadd_rn(acc[c], __ldg(row + c));
+            for (int c = 0; c < CMAX; c++)
+                if (c < C) acc[c] = __fadd_rn(tt == 0 ? 0.0f : acc[c], __ldg(row + c));
+        }
     }
+    auto acc_of = [&](int c) { return acc[c]; };
     double sum = 0.0;
 #pragma unroll
     for (int c = 0; c < CMAX; c++)
-        if (c < C) sum = __dadd_rn(sum, static_cast<double>(acc[c]));
+        if (c < C) sum = __dadd_rn(sum, static_cast<double>(acc_of(c)));
     // RN(acc / sum) from the correctly rounded reciprocal with one correction step (Markstein,
     // IBM J. Res. Dev. 34(1), 1990): q = RN(a y), r = a - q sum exactly by FMA, RN(q + r y)
     const double inv = __drcp_rn(sum);
@@ -110,7 +128,7 @@ classify_kernel(const PackedNode* __restrict__ nodes, const int* __restrict__ tr
 #pragma unroll
     for (int c = 0; c < CMAX; c++) {
         if (c < C) {
-            const double a = static_cast<double>(acc[c]);
+            const double a = static_cast<double>(acc_of(c));
             const double q = __dmul_rn(a, inv);
             const double q1 = __fma_rn(__fma_rn(-q, sum, a), inv, q);
             const float v = __double2float_rn(q1);
@@ -196,21 +214,22 @@ __global__ void plain_argmax_kernel(const float* __restrict__ probs, int C, long
 template <int CMAX>
 void launch_classify(cf_context* ctx, cudaStream_t stream, const cf_forest* f, const FrameDesc* frames, int num_frames,
                      int blocks) {
-    const size_t smem = sizeof(PackedNode) * f->num_trees * f->cache_per_tree;
+    const size_t smem = sizeof(PackedNode) * f->num_trees * f->cache_per_tree +
+                        sizeof(uint32_t) * std::min(f->num_trees, kTreeChunk) * kClassifyThreads;
+    auto kernel = classify_kernel<CMAX>;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CF_CUDA_CHECK(cudaStreamIsCapturing(stream, &cs));
     if (cs == cudaStreamCaptureStatusNone)   // set before capture (an uncaptured pass runs first)
-        CF_CUDA_CHECK(cudaFuncSetAttribute(classify_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CF_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(std::max<size_t>(smem, 1))));
-    launch_on(ctx, stream, "classify", dim3(blocks), dim3(kClassifyThreads), smem, classify_kernel<CMAX>, f->nodes.get(),
-           f->d_tree_base.get(), f->num_trees, f->cache_per_tree, f->leaves.get(), f->C, frames, num_frames);
+    launch_on(ctx, stream, "classify", dim3(blocks), dim3(kClassifyThreads), smem, kernel, f->nodes.get(),
+              f->d_tree_base.get(), f->num_trees, f->cache_per_tree, f->leaves.get(), f->C, frames, num_frames);
 }
 
 }  // namespace
 
 int classify_blocks_for(int width, int height) {
-    const long long plane = static_cast<long long>(width) * height;
-    return static_cast<int>((plane + kClassifyThreads - 1) / kClassifyThreads);
+    return ((width + kTileW - 1) / kTileW) * ((height + kTileH - 1) / kTileH);
 }
 
 void classify_frames(cf_context* ctx, const cf_forest* forest, const FrameDesc* frames_dev, int num_frames,
@@ -460,6 +479,61 @@ cf_status cf_predict_dataset_plain(cf_forest* forest, cf_dataset* ds, int first,
             launch(ctx, "plain_normalize", dim3(blocks), dim3(256), 0, plain_normalize_kernel, fr.probs, C, plane);
             CF_CUDA_CHECK(cudaStreamSynchronize(st));
             launch(ctx, "plain_argmax", dim3(blocks), dim3(256), 0, plain_argmax_kernel, fr.probs, C, plane, fr.labels);
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+        }
+    });
+}
+
+cf_status cf_predict_host_plain(cf_forest* forest, int count, int width, int height, const uint8_t* rgb,
+                                const uint16_t* depth_mm, float* probabilities, uint8_t* labels) {
+    return guard([&] {
+        CF_REQUIRE(forest && rgb && depth_mm, "cf_predict_host_plain: NULL argument");
+        CF_REQUIRE(count >= 1 && width >= 1 && height >= 1, "cf_predict_host_plain: empty input");
+        cf_context* ctx = forest->ctx;
+        make_current(ctx);
+        const int C = forest->C;
+        const size_t plane = static_cast<size_t>(width) * height;
+        const unsigned blocks = static_cast<unsigned>((plane + 255) / 256);
+        forest->raw_rgb.reserve(plane * 3);
+        forest->raw_depth.reserve(plane);
+        forest->color.reserve(plane * 3);
+        forest->depth.reserve(plane);
+        forest->probs.reserve(plane * C);
+        forest->labels.reserve(plane);
+        // the reference copies the probabilities back for every image, requested or not
+        std::vector<float> host_probs(probabilities ? 0 : plane * C);
+        std::vector<uint8_t> host_labels(labels ? 0 : plane);
+        cudaStream_t st = ctx->stream;
+        for (int i = 0; i < count; i++) {
+            CF_CUDA_CHECK(cudaMemcpyAsync(forest->raw_rgb.get(), rgb + plane * 3 * i, plane * 3, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(forest->raw_depth.get(), depth_mm + plane * i, plane * 2, cudaMemcpyHostToDevice,
+                                          st));
+            integrate_frames(ctx, forest->raw_rgb.get(), forest->raw_depth.get(), 1, width, height, forest->color.get(),
+                             forest->depth.get());
+            FrameDesc fr;
+            fr.color = forest->color.get();
+            fr.depth = forest->depth.get();
+            fr.probs = forest->probs.get();
+            fr.labels = forest->labels.get();
+            fr.width = width;
+            fr.height = height;
+            fr.first_block = 0;
+            fr.pad = 0;
+            CF_CUDA_CHECK(cudaMemsetAsync(fr.probs, 0, sizeof(float) * C * plane, st));
+            for (int t = 0; t < forest->num_trees; t++) {
+                launch(ctx, "plain_classify", dim3(blocks), dim3(256), 0, plain_classify_tree_kernel, forest->nodes.get(),
+                       forest->tree_base[t], forest->leaves.get(), C, fr);
+                CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            }
+            const long long pl = static_cast<long long>(plane);
+            launch(ctx, "plain_normalize", dim3(blocks), dim3(256), 0, plain_normalize_kernel, fr.probs, C, pl);
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            launch(ctx, "plain_argmax", dim3(blocks), dim3(256), 0, plain_argmax_kernel, fr.probs, C, pl, fr.labels);
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            float* pd = probabilities ? probabilities + plane * C * i : host_probs.data();
+            uint8_t* ld = labels ? labels + plane * i : host_labels.data();
+            CF_CUDA_CHECK(cudaMemcpyAsync(pd, fr.probs, sizeof(float) * plane * C, cudaMemcpyDeviceToHost, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(ld, fr.labels, plane, cudaMemcpyDeviceToHost, st));
             CF_CUDA_CHECK(cudaStreamSynchronize(st));
         }
     });

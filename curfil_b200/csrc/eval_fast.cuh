@@ -57,6 +57,14 @@ __device__ __forceinline__ int fast_norm(int v, float av, float d, float inv_d) 
     return v < 0 ? -r : r;
 }
 
+// Normalisation policies of feature_bin.
+// CheckedNorm: fast_norm, each value checked on its own.
+struct CheckedNorm {
+    __device__ __forceinline__ int operator()(int v, float av, float d, float inv_d) const {
+        return fast_norm(v, av, d, inv_d);
+    }
+};
+
 // trunc(RN(v / d)) for an int parameter (used outside the hot loop)
 __device__ __forceinline__ int fast_norm(int v, float d, float inv_d) {
     return fast_norm(v, static_cast<float>(v < 0 ? -v : v), d, inv_d);
@@ -156,22 +164,22 @@ struct ThresholdSide {
     __device__ __forceinline__ int exact(double r) const { return r <= static_cast<double>(thr) ? 0 : 1; }
 };
 
-template <typename Bins>
+template <typename Bins, typename Norm = CheckedNorm>
 __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, const EvalFeat& f, bool flip,
-                                           const Bins& bins) {
+                                           const Bins& bins, const Norm& norm = Norm()) {
     const int T = bins.nan();
     if (!(p.d > 0.0f)) return T;
     const int o1x = flip ? -f.v[0] : f.v[0];
     const int o2x = flip ? -f.v[2] : f.v[2];
-    const int x1 = p.x + fast_norm(o1x, f.av[0], p.d, p.inv_d);
-    const int y1 = p.y + fast_norm(f.v[1], f.av[1], p.d, p.inv_d);
-    const int w1 = max(1, fast_norm(f.v[4], f.av[4], p.d, p.inv_d));
-    const int h1 = max(1, fast_norm(f.v[5], f.av[5], p.d, p.inv_d));
+    const int x1 = p.x + norm(o1x, f.av[0], p.d, p.inv_d);
+    const int y1 = p.y + norm(f.v[1], f.av[1], p.d, p.inv_d);
+    const int w1 = max(1, norm(f.v[4], f.av[4], p.d, p.inv_d));
+    const int h1 = max(1, norm(f.v[5], f.av[5], p.d, p.inv_d));
     if (x1 - w1 < 0 || x1 + w1 >= W || y1 - h1 < 0 || y1 + h1 >= H) return T;
-    const int x2 = p.x + fast_norm(o2x, f.av[2], p.d, p.inv_d);
-    const int y2 = p.y + fast_norm(f.v[3], f.av[3], p.d, p.inv_d);
-    const int w2 = max(1, fast_norm(f.v[6], f.av[6], p.d, p.inv_d));
-    const int h2 = max(1, fast_norm(f.v[7], f.av[7], p.d, p.inv_d));
+    const int x2 = p.x + norm(o2x, f.av[2], p.d, p.inv_d);
+    const int y2 = p.y + norm(f.v[3], f.av[3], p.d, p.inv_d);
+    const int w2 = max(1, norm(f.v[6], f.av[6], p.d, p.inv_d));
+    const int h2 = max(1, norm(f.v[7], f.av[7], p.d, p.inv_d));
     if (x2 - w2 < 0 || x2 + w2 >= W || y2 - h2 < 0 || y2 + h2 >= H) return T;
     const int ul1 = (y1 - h1) * W + (x1 - w1), ur1 = (y1 - h1) * W + (x1 + w1);
     const int ll1 = (y1 + h1) * W + (x1 - w1), lr1 = (y1 + h1) * W + (x1 + w1);

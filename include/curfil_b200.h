@@ -271,6 +271,12 @@ cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, c
  * batched form is measured against. DEVICE pointers, either may be NULL. */
 cf_status cf_predict_dataset_plain(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
                                    uint8_t* labels);
+/* The plain form from raw host frames as RandomForestImage::predict runs it on the GPU
+ * (random_forest_image.cpp:258-301): per image, upload and integral images, the launches above,
+ * then the full probabilities [C][H][W] and the labels copied back to the host (the probabilities
+ * are copied even when `probabilities` is NULL, as there). HOST pointers. */
+cf_status cf_predict_host_plain(cf_forest* forest, int count, int width, int height, const uint8_t* rgb,
+                                const uint16_t* depth_mm, float* probabilities, uint8_t* labels);
 
 /* A fixed batch of `count` raw frames (width x height) captured once as a CUDA graph: host-to-device
  * copy from pinned staging buffers, integral images, classification, results back to pinned buffers.

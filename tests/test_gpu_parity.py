@@ -361,6 +361,17 @@ def test_predict_batched_equals_plain_per_image(ctx, scene, forest_and_oracle):
     np.testing.assert_array_equal(la.cpu().numpy(), lb.cpu().numpy())
 
 
+def test_predict_host_plain_equals_batched(ctx, forest_and_oracle):
+    forest, _, _ = forest_and_oracle
+    rgb, depth, _ = H.frames(seed=321, n=2, w=96, h=72, cells=12, classes=40)
+    p1, l1 = forest.predict(rgb, depth)
+    p2, l2 = forest.predict_plain(rgb, depth)
+    np.testing.assert_array_equal(p1.view(np.uint32), p2.view(np.uint32))
+    np.testing.assert_array_equal(l1, l2)
+    _, l3 = forest.predict_plain(rgb, depth, probabilities=False)
+    np.testing.assert_array_equal(l1, l3)
+
+
 def test_predict_graph_equals_host_path(ctx, forest_and_oracle):
     forest, _, _ = forest_and_oracle
     g = cf.PredictGraph(forest, 3, 96, 72, probabilities=True)
