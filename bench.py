@@ -362,6 +362,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-per-node", action="store_true", help="skip the plain per-node comparison tree")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default split-search launch shape")
     # workload size (defaults: the full-size configuration); smaller cases are for profiler captures
     ap.add_argument("--images", type=int, default=W["images"])
     ap.add_argument("--trees", type=int, default=W["trees"])
@@ -423,6 +424,12 @@ def main():
     ds = cf.Dataset.from_raw(ctx, rgb, depth)
     tree_ids = [rank * W["trees"] + t for t in range(W["trees"])]
     per_tree = tree_samples(labels, depth, cfg, tree_ids)
+    # the split search's launch shape, chosen by the autotuner on this rank's first tree (untimed)
+    autotune = None
+    if not args.tuning and not args.no_autotune:
+        t0_, s0_, _, c0_ = per_tree[0]
+        autotune = cf.autotune_split_search(ds, s0_, W["classes"], cfg, tree_id=t0_, seed_counter=c0_)
+        autotune.pop("key", None)
 
     def step():
         trees, evals = [], 0
@@ -534,7 +541,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": dict(workload_config(), parallelism="trees sharded over %d GPU(s)" % world,
-                               split_search_tuning=ctx.get_tuning().as_dict()),
+                               split_search_tuning=ctx.get_tuning().as_dict(), autotune=autotune),
                 "roofline": {"bound": "hbm", "kernel": "level_eval", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                              "peak_source": peak_kind, "bytes_per_eval": bytes_per_eval,

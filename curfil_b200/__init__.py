@@ -158,6 +158,14 @@ class Context:
     def launch_count(self):
         return lib().cf_context_launch_count(self.handle)
 
+    def device(self):
+        """{'name', 'sms', 'cc'} of the context's device."""
+        name = ctypes.create_string_buffer(256)
+        sms, major, minor = _i32(), _i32(), _i32()
+        _check(lib().cf_context_device(self.handle, name, 256, ctypes.byref(sms), ctypes.byref(major),
+                                       ctypes.byref(minor)))
+        return {"name": name.value.decode(), "sms": sms.value, "cc": "%d.%d" % (major.value, minor.value)}
+
     def get_tuning(self):
         t = EvalTuning()
         _check(lib().cf_context_get_tuning(self.handle, ctypes.byref(t)))
@@ -425,6 +433,41 @@ def train_tree(ds, samples, num_classes, config, tree_id=0, seed_counter=0, mode
     _check(lib().cf_train_tree(ds.handle, len(samples), _p(samples), int(num_classes), ctypes.byref(config),
                                int(tree_id), ctypes.byref(sc), int(mode), ctypes.byref(h)))
     return Tree(h), sc.value
+
+
+def autotune_split_search(ds, samples, num_classes, config, tree_id=0, seed_counter=0, repeats=1, cache=None):
+    """Choose the split search's launch shape for this workload (cf_autotune_split_search) and set it on
+    the dataset's context. With `cache` (a JSON file path) a previous choice for the same device and
+    workload signature is reused without measuring. Returns a dict with the shape and timings."""
+    import json
+    samples = np.ascontiguousarray(samples, SAMPLE_DTYPE)
+    ctx = ds.ctx
+    dev = ctx.device()
+    key = "%s/%dSM|C=%d F=%d T=%d depth=%d N=%d frames=%dx%dx%d" % (
+        dev["name"], dev["sms"], num_classes, config.feature_count, config.thresholds, config.max_depth,
+        len(samples), ds.n, ds.width, ds.height)
+    table = {}
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            table = json.load(f)
+        if key in table:
+            ctx.set_tuning(**table[key]["tuning"])
+            return dict(table[key], key=key, from_cache=True)
+    best = EvalTuning()
+    best_ms, start_ms, trials = ctypes.c_double(), ctypes.c_double(), _i32()
+    _check(lib().cf_autotune_split_search(ds.handle, len(samples), _p(samples), int(num_classes),
+                                          ctypes.byref(config), int(tree_id), _i32(seed_counter), int(repeats),
+                                          ctypes.byref(best), ctypes.byref(best_ms), ctypes.byref(start_ms),
+                                          ctypes.byref(trials)))
+    entry = {"tuning": best.as_dict(), "split_search_ms": best_ms.value, "start_ms": start_ms.value,
+             "trials": trials.value}
+    if cache:
+        table[key] = entry
+        tmp = cache + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache)
+    return dict(entry, key=key, from_cache=False)
 
 
 def forest_seed(random_seed):

@@ -187,6 +187,22 @@ cf_status cf_context_reset_timing(cf_context* ctx) {
 
 int64_t cf_context_launch_count(cf_context* ctx) { return ctx ? ctx->launches.load() : 0; }
 
+cf_status cf_context_device(cf_context* ctx, char* name, size_t name_length, int* num_sms, int* cc_major,
+                            int* cc_minor) {
+    return cf::guard([&] {
+        CF_REQUIRE(ctx, "cf_context_device: ctx is NULL");
+        cudaDeviceProp prop;
+        CF_CUDA_CHECK(cudaGetDeviceProperties(&prop, ctx->device));
+        if (name && name_length > 0) {
+            std::strncpy(name, prop.name, name_length - 1);
+            name[name_length - 1] = '\0';
+        }
+        if (num_sms) *num_sms = prop.multiProcessorCount;
+        if (cc_major) *cc_major = prop.major;
+        if (cc_minor) *cc_minor = prop.minor;
+    });
+}
+
 cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out) {
     return cf::guard([&] {
         CF_REQUIRE(ctx && out, "cf_context_get_tuning: NULL argument");

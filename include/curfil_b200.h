@@ -100,6 +100,9 @@ cf_status cf_context_kernel_time(cf_context* ctx, const char* kernel, double* to
 cf_status cf_context_reset_timing(cf_context* ctx);
 /* Number of kernel launches issued by this context since creation. */
 int64_t cf_context_launch_count(cf_context* ctx);
+/* Name, SM count and compute capability of the context's device (e.g. to key tuning caches). */
+cf_status cf_context_device(cf_context* ctx, char* name, size_t name_length, int* num_sms, int* cc_major,
+                            int* cc_minor);
 
 /* Launch shape of the level-batched split search used by every training call on this context.
  * Project extension with no reference counterpart (the reference's launch shapes are compile-time
@@ -116,6 +119,16 @@ typedef struct cf_eval_tuning {
 } cf_eval_tuning;
 cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out);
 cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning);
+/* Project-written autotuner (no reference counterpart): trains the given tree (as cf_train_tree,
+ * level-batched) under candidate launch shapes, starting from the context's current one, by
+ * coordinate descent over bins_budget_words, items_per_slot, feature_granule and features_per_tile,
+ * timing the split search with the trainer's CUDA events (min over `repeats`). Every candidate must
+ * yield the identical tree (else CF_ERR_STATE). The fastest shape is set on the context and returned
+ * with its time; `start_ms` is the time of the starting shape, `trials` the shapes measured (either
+ * may be NULL). On error the context keeps its previous shape. */
+cf_status cf_autotune_split_search(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                                   const cf_train_config* config, int tree_id, int32_t seed_counter, int repeats,
+                                   cf_eval_tuning* best, double* best_ms, double* start_ms, int* trials);
 
 /* ---------------------------------------------------------------------------------------------
  * Datasets: integral images resident in device memory

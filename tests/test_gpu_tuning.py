@@ -89,6 +89,30 @@ def test_tuning_changes_speed_not_results(ctx, scene):
         ctx.set_tuning()
 
 
+def test_autotune_keeps_the_tree_and_caches(ctx, scene, tmp_path):
+    samples, _ = H.class_uniform_samples(scene["labels"], scene["depth"], 40, 40)
+    cfg = cf.TrainConfig(feature_count=64, thresholds=10, max_depth=6, min_sample_count=4, box_radius=40,
+                         region_size=10)
+    ctx.set_tuning()
+    before, _ = cf.train_tree(scene["ds"], samples, 40, cfg, seed_counter=3)
+    cache = str(tmp_path / "tuning.json")
+    try:
+        r = cf.autotune_split_search(scene["ds"], samples, 40, cfg, seed_counter=3, cache=cache)
+        assert not r["from_cache"] and r["trials"] >= 10
+        assert r["split_search_ms"] <= r["start_ms"]
+        assert ctx.get_tuning().as_dict() == r["tuning"]
+        after, _ = cf.train_tree(scene["ds"], samples, 40, cfg, seed_counter=3)
+        A, B = before.arrays(), after.arrays()
+        for k in A:
+            np.testing.assert_array_equal(A[k], B[k], err_msg=k)
+        ctx.set_tuning()
+        again = cf.autotune_split_search(scene["ds"], samples, 40, cfg, seed_counter=3, cache=cache)
+        assert again["from_cache"] and again["tuning"] == r["tuning"]
+        assert ctx.get_tuning().as_dict() == r["tuning"]
+    finally:
+        ctx.set_tuning()
+
+
 @pytest.mark.parametrize("T", [31, 32, 45])
 def test_counts_bit_exact_around_search_padding(ctx, scene, T):
     """T <= 31 takes the branch-free search over 32 padded positions, larger T the generic one."""
