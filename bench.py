@@ -360,7 +360,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-per-node", action="store_true", help="skip the plain per-node comparison tree")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default split-search launch shape")
     # workload size (defaults: the full-size configuration); smaller cases are for profiler captures
@@ -488,24 +488,32 @@ def main():
         for t in ptrees:
             t.close()
 
-    # end to end through cf_forest_train with host buffers
-    e2e = None
-    if args.e2e_steps > 0:
+    # end to end through cf_forest_train with host buffers: frames in, trees out
+    def forest_e2e(sampler, steps):
+        c = train_config()
+        c.sampler = sampler
         t0 = time.perf_counter()
         e2e_evals = 0
         d2h = 0
-        for _ in range(args.e2e_steps):
-            ts = cf.train_forest(ctx, rgb, depth, labels, W["classes"], cfg, W["trees"])
+        for _ in range(steps):
+            ts = cf.train_forest(ctx, rgb, depth, labels, W["classes"], c, W["trees"])
             for t in ts:
                 e2e_evals += t.train_stats()[0]
                 d2h += t.num_nodes * (4 * 4 + 11 + 4 + 8 + 4 * W["classes"])
-        e2e_s = time.perf_counter() - t0
-        e2e_s = max_over_ranks(e2e_s)
-        e2e = {"value": sum_over_ranks(e2e_evals) / e2e_s, "unit": "feature-evals/s",
-               "h2d_bytes_per_step": int(rgb.nbytes + depth.nbytes),
-               "d2h_bytes_per_step": int(d2h / args.e2e_steps),
-               "note": "cf_forest_train: upload, GPU integral images, host class-uniform sampling (one thread, "
-                       "as the reference's reproducible mode), level-batched training, tree download"}
+                t.close()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        h2d = rgb.nbytes + depth.nbytes + (labels.nbytes + depth.nbytes if sampler == 1 else 0)
+        return {"value": sum_over_ranks(e2e_evals) / e2e_s, "unit": "feature-evals/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h / steps)}
+
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = forest_e2e(1, args.e2e_steps)
+        e2e["note"] = ("cf_forest_train: frames and labels uploaded, GPU integral images, device class-uniform "
+                       "sampling, level-batched training, trees downloaded")
+        e2e["reference_sampler"] = forest_e2e(0, 1)
+        e2e["reference_sampler"]["note"] = ("the same with the reference's class-uniform reservoir on one host "
+                                            "thread (its RNG streams)")
 
     # the plain per-node form (reference-structured kernels: responses to HBM, one block per
     # (threshold, feature), score kernel, host argmax, node by node) on this rank's first tree:

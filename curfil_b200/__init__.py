@@ -38,7 +38,7 @@ class TrainConfig(ctypes.Structure):
                 ("feature_count", ctypes.c_uint32), ("min_sample_count", ctypes.c_uint32),
                 ("max_depth", ctypes.c_int32), ("box_radius", ctypes.c_uint16),
                 ("region_size", ctypes.c_uint16), ("thresholds", ctypes.c_uint16),
-                ("reserved0", ctypes.c_uint16), ("num_threads", ctypes.c_int32),
+                ("sampler", ctypes.c_uint16), ("num_threads", ctypes.c_int32),
                 ("max_images", ctypes.c_int32), ("image_cache_size", ctypes.c_int32),
                 ("max_samples_per_batch", ctypes.c_uint32), ("acceleration_mode", ctypes.c_int32),
                 ("use_cie_lab", ctypes.c_int32), ("use_depth_filling", ctypes.c_int32),
@@ -477,8 +477,9 @@ def forest_seed(random_seed):
     return s.value
 
 
-def sample_tree_pixels(labels, depth_mm, num_classes, config, num_trees, seed_counter, ignored=None):
-    """Training pixels of one tree (sampling + block sort). Returns (samples, prior, new seed counter)."""
+def sample_tree_pixels(labels, depth_mm, num_classes, config, num_trees, seed_counter, ignored=None, ctx=None):
+    """Training pixels of one tree (sampling + block sort). Returns (samples, prior, new seed counter).
+    With `ctx`, classUniform sampling runs on that context's device (cf_sample_tree_pixels_device)."""
     labels = np.ascontiguousarray(labels, np.uint8)
     depth_mm = np.ascontiguousarray(depth_mm, np.uint16)
     n, h, w = labels.shape
@@ -489,9 +490,14 @@ def sample_tree_pixels(labels, depth_mm, num_classes, config, num_trees, seed_co
     cap = n * (config.samples_per_image // max(1, num_trees)) + num_classes
     out = np.empty(cap, SAMPLE_DTYPE)
     prior = np.empty(num_classes, np.uint32)
-    _check(lib().cf_sample_tree_pixels(n, w, h, _p(labels), _p(depth_mm), int(num_classes), _p(ign),
-                                       ctypes.byref(config), int(num_trees), ctypes.byref(sc), _p(out),
-                                       ctypes.c_int64(len(out)), ctypes.byref(cnt), _p(prior)))
+    if ctx is not None:
+        _check(lib().cf_sample_tree_pixels_device(ctx.handle, n, w, h, _p(labels), _p(depth_mm), int(num_classes),
+                                                  _p(ign), ctypes.byref(config), int(num_trees), ctypes.byref(sc),
+                                                  _p(out), ctypes.c_int64(len(out)), ctypes.byref(cnt), _p(prior)))
+    else:
+        _check(lib().cf_sample_tree_pixels(n, w, h, _p(labels), _p(depth_mm), int(num_classes), _p(ign),
+                                           ctypes.byref(config), int(num_trees), ctypes.byref(sc), _p(out),
+                                           ctypes.c_int64(len(out)), ctypes.byref(cnt), _p(prior)))
     return out[:cnt.value].copy(), prior, sc.value
 
 

@@ -10,9 +10,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <memory>
 
 #include "host_rng.h"
+#include "sampling.h"
 #include "tree.h"
 
 namespace cf {
@@ -134,10 +136,13 @@ void block_sort(std::vector<cf_sample>& s) {
 // Training pixels of one tree as RandomForestImage::train / RandomTreeImage::train draw them:
 // image reservoir (maxImages), class prior, sampling, block sort. Sample image indices refer to
 // the dataset. `rs` is the tree's random source (seed SEED + treeId).
+// With `frames` (config.sampler == 1, classUniform) the class prior and the sampling run on the
+// device (sample_class_uniform_device).
 std::vector<cf_sample> sample_tree(int num_images, int width, int height, const uint8_t* labels,
                                    const uint16_t* depth_mm, int num_classes, const uint8_t* ignored,
                                    const cf_train_config& config, int num_trees, RandomSource& rs,
-                                   std::vector<uint32_t>& prior) {
+                                   std::vector<uint32_t>& prior, cf_context* ctx = nullptr,
+                                   DeviceFrames* frames = nullptr) {
     const size_t plane = static_cast<size_t>(width) * height;
     std::vector<int> images(num_images);
     for (int i = 0; i < num_images; i++) images[i] = i;
@@ -156,6 +161,15 @@ std::vector<cf_sample> sample_tree(int num_images, int width, int height, const 
         }
         images = res;
     }
+    const int subsample = static_cast<int>(config.samples_per_image / static_cast<uint32_t>(num_trees));
+    CF_REQUIRE(subsample > 0, "samplesPerImage / treeCount must be > 0");
+    const uint8_t flip = config.horizontal_flipping ? 2 : 0;
+    if (frames && config.sampler == 1 && config.subsampling_type == 0) {
+        std::vector<cf_sample> samples = sample_class_uniform_device(ctx, *frames, images, depth_mm, num_classes,
+                                                                     ignored, subsample, rs, flip, &prior);
+        for (auto& s : samples) s.image = static_cast<uint32_t>(images[s.image]);
+        return samples;
+    }
     // calculateLabelPriorDistribution (random_tree_image.cpp:885-909)
     prior.assign(num_classes, 0);
     for (int img : images)
@@ -164,9 +178,6 @@ std::vector<cf_sample> sample_tree(int num_images, int width, int height, const 
             CF_REQUIRE(l < num_classes, "label image holds a label >= number of classes");
             prior[l]++;
         }
-    const int subsample = static_cast<int>(config.samples_per_image / static_cast<uint32_t>(num_trees));
-    CF_REQUIRE(subsample > 0, "samplesPerImage / treeCount must be > 0");
-    const uint8_t flip = config.horizontal_flipping ? 2 : 0;
     std::vector<cf_sample> samples =
         config.subsampling_type == 0
             ? sample_class_uniform(images, width, height, labels, depth_mm, num_classes, ignored, subsample, rs, flip)
@@ -213,6 +224,35 @@ cf_status cf_sample_tree_pixels(int num_images, int width, int height, const uin
     });
 }
 
+cf_status cf_sample_tree_pixels_device(cf_context* ctx, int num_images, int width, int height, const uint8_t* labels,
+                                       const uint16_t* depth_mm, int num_classes, const uint8_t* ignored,
+                                       const cf_train_config* config, int num_trees, int32_t* seed_counter,
+                                       cf_sample* out, int64_t capacity, int64_t* count, uint32_t* prior) {
+    return guard([&] {
+        CF_REQUIRE(ctx && labels && depth_mm && config && seed_counter && count,
+                   "cf_sample_tree_pixels_device: NULL argument");
+        CF_REQUIRE(num_images >= 1 && width >= 1 && height >= 1, "cf_sample_tree_pixels_device: empty input");
+        CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_sample_tree_pixels_device: classes must be in [1, 256]");
+        CF_REQUIRE(num_trees >= 1, "cf_sample_tree_pixels_device: need at least one tree");
+        CF_REQUIRE(config->subsampling_type == 0, "cf_sample_tree_pixels_device: classUniform sampling only");
+        make_current(ctx);
+        DeviceFrames frames;
+        frames.upload(ctx, num_images, width, height, labels, depth_mm);
+        cf_train_config cfg = *config;
+        cfg.sampler = 1;
+        RandomSource rs(seed_counter);
+        std::vector<uint32_t> pr;
+        std::vector<cf_sample> s = sample_tree(num_images, width, height, labels, depth_mm, num_classes, ignored, cfg,
+                                               num_trees, rs, pr, ctx, &frames);
+        *count = static_cast<int64_t>(s.size());
+        if (out) {
+            CF_REQUIRE(capacity >= static_cast<int64_t>(s.size()), "cf_sample_tree_pixels_device: output buffer too small");
+            std::memcpy(out, s.data(), sizeof(cf_sample) * s.size());
+        }
+        if (prior) std::memcpy(prior, pr.data(), sizeof(uint32_t) * pr.size());
+    });
+}
+
 cf_status cf_forest_train(cf_context* ctx, int num_images, int width, int height, const uint8_t* rgb,
                           const uint16_t* depth_mm, const uint8_t* labels, int num_classes, const uint8_t* ignored,
                           const cf_train_config* config, int num_trees, int mode, cf_tree** trees) {
@@ -240,16 +280,36 @@ cf_status cf_forest_train(cf_context* ctx, int num_images, int width, int height
             const cf_status st = cf_forest_seed(config->random_seed, &SEED);
             if (st != CF_OK) fail(st, "cf_forest_train: seed");
         }
+        CF_REQUIRE(config->sampler == 0 || config->sampler == 1, "unknown sampler");
+        std::unique_ptr<DeviceFrames> frames;
+        if (config->sampler == 1 && config->subsampling_type == 0) {
+            frames.reset(new DeviceFrames());
+            frames->upload(ctx, num_images, width, height, labels, depth_mm);
+        }
+        // the training pixels of tree t + 1 are drawn on a host thread (and the sampler's own stream)
+        // while tree t trains
+        struct Drawn {
+            std::vector<cf_sample> samples;
+            std::vector<uint32_t> prior;
+            int32_t counter = 0;
+        };
+        auto draw = [&](int t) {
+            CF_CUDA_CHECK(cudaSetDevice(ctx->device));
+            Drawn d;
+            d.counter = SEED + t;
+            RandomSource rs(&d.counter);
+            d.samples = sample_tree(num_images, width, height, labels, depth_mm, num_classes, ignored, *config,
+                                    num_trees, rs, d.prior, ctx, frames.get());
+            return d;
+        };
         try {
+            std::future<Drawn> next = std::async(std::launch::async, draw, 0);
             for (int t = 0; t < num_trees; t++) {
-                int32_t counter = SEED + t;
-                RandomSource rs(&counter);
-                std::vector<uint32_t> prior;
-                std::vector<cf_sample> samples = sample_tree(num_images, width, height, labels, depth_mm, num_classes,
-                                                             ignored, *config, num_trees, rs, prior);
-                cf_tree* tree = train_tree(ds.get(), samples.data(), static_cast<int>(samples.size()), num_classes,
-                                           *config, t, &counter, mode);
-                tree->prior = prior;
+                Drawn cur = next.get();
+                if (t + 1 < num_trees) next = std::async(std::launch::async, draw, t + 1);
+                cf_tree* tree = train_tree(ds.get(), cur.samples.data(), static_cast<int>(cur.samples.size()),
+                                           num_classes, *config, t, &cur.counter, mode);
+                tree->prior = cur.prior;
                 trees[t] = tree;
             }
         } catch (...) {

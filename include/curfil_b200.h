@@ -69,7 +69,9 @@ typedef struct cf_train_config {
     uint16_t box_radius;        /* offset range ("boxRadius") */
     uint16_t region_size;       /* box half-size range ("regionSize") */
     uint16_t thresholds;
-    uint16_t reserved0;
+    uint16_t sampler;           /* cf_forest_train's classUniform sampler: 0 the reference's reservoir on the
+                                   host (its RNG streams, one thread), 1 the device sampler of
+                                   cf_sample_tree_pixels_device (project extension, deterministic) */
     int32_t num_threads;
     int32_t max_images;
     int32_t image_cache_size;
@@ -239,6 +241,17 @@ cf_status cf_sample_tree_pixels(int num_images, int width, int height, const uin
                                 const uint16_t* depth_mm, int num_classes, const uint8_t* ignored,
                                 const cf_train_config* config, int num_trees, int32_t* seed_counter,
                                 cf_sample* out, int64_t capacity, int64_t* count, uint32_t* prior);
+/* The same on the device for classUniform (project extension; the reference's sampler is not
+ * reproducible with several threads). Each eligible pixel (label not ignored, depth > 0) at
+ * position k of the tree's image list and pixel p gets the key Philox4x32-10(key = (s, 0x53414D50),
+ * counter = (k*H*W + p, 0, 0, 0)) word 0, s being the draw the reference's sampler takes from the
+ * tree's RandomSource; every class keeps its per-class quota of pixels with the smallest
+ * (key, k*H*W + p); samples are ordered by (image, label, y/10, x/10, y, x). Host inputs; the
+ * seed counter advances as for cf_sample_tree_pixels. */
+cf_status cf_sample_tree_pixels_device(cf_context* ctx, int num_images, int width, int height, const uint8_t* labels,
+                                       const uint16_t* depth_mm, int num_classes, const uint8_t* ignored,
+                                       const cf_train_config* config, int num_trees, int32_t* seed_counter,
+                                       cf_sample* out, int64_t capacity, int64_t* count, uint32_t* prior);
 /* RandomTree accessors (random_tree.h:499-1003). */
 cf_status cf_tree_info(cf_tree* tree, int* num_nodes, int* num_classes, int* depth, int* tree_id);
 /* Node arrays in breadth-first id order (index = nodeId - treeId); any pointer may be NULL.

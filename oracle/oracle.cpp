@@ -819,4 +819,60 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
     return static_cast<int>(all.size());
 }
 
+/* The device classUniform sampler's definition (curfil_b200 cf_sample_tree_pixels_device): keys
+ * from Philox4x32-10 per eligible pixel, the per-class quota of smallest (key, pixel index), order
+ * (image, label, y/10, x/10, y, x). Same seed draws as the reservoir sampler above. */
+int orc_sample_class_uniform_keys(int n, int width, int height, const uint8_t* labels, const uint16_t* depth_mm,
+                                  int num_classes, const uint8_t* ignore, int subsample_count, int* seed_counter,
+                                  int capacity, orc_sample* out) {
+    int numLabels = num_classes;
+    for (int c = 0; c < num_classes; c++)
+        if (ignore[c]) numLabels--;
+    const size_t samplesPerClass =
+        static_cast<size_t>(std::ceil(n * static_cast<double>(subsample_count) / static_cast<double>(numLabels)));
+    Sampler seedSampler = uniform_sampler(seed_counter, 0xFFFFFF);
+    const uint32_t k0 = static_cast<uint32_t>(seedSampler.next());
+    (void)uniform_sampler(seed_counter, 0x7FFFFFFF);
+    const size_t hw = static_cast<size_t>(width) * height;
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> keys(num_classes);   // (key, pixel index)
+    for (size_t i = 0; i < n * hw; i++) {
+        const uint8_t label = labels[i];
+        if (label >= num_classes || ignore[label] || depth_mm[i] == 0) continue;
+        uint32_t c[4] = {static_cast<uint32_t>(i), 0u, 0u, 0u};
+        philox4x32_10(k0, 0x53414D50u, c);
+        keys[label].emplace_back(c[0], static_cast<uint32_t>(i));
+    }
+    std::vector<orc_sample> all;
+    for (int label = 0; label < num_classes; label++) {
+        if (ignore[label]) continue;
+        auto& v = keys[label];
+        if (v.size() < samplesPerClass) return -1;
+        std::sort(v.begin(), v.end());
+        for (size_t j = 0; j < samplesPerClass; j++) {
+            const size_t i = v[j].second;
+            const size_t img = i / hw, p = i % hw;
+            orc_sample s;
+            s.x = static_cast<uint16_t>(p % width);
+            s.y = static_cast<uint16_t>(p / width);
+            s.image = static_cast<uint32_t>(img);
+            s.depth = static_cast<float>(static_cast<int>(depth_mm[i])) / 1000.0f;
+            s.label = static_cast<uint8_t>(label);
+            s.flip = 0;
+            s.reserved = 0;
+            all.push_back(s);
+        }
+    }
+    std::sort(all.begin(), all.end(), [](const orc_sample& a, const orc_sample& b) {
+        if (a.image != b.image) return a.image < b.image;
+        if (a.label != b.label) return a.label < b.label;
+        if (a.y / 10 != b.y / 10) return a.y / 10 < b.y / 10;
+        if (a.x / 10 != b.x / 10) return a.x / 10 < b.x / 10;
+        if (a.y != b.y) return a.y < b.y;
+        return a.x < b.x;
+    });
+    if (static_cast<int>(all.size()) > capacity) return -2;
+    std::copy(all.begin(), all.end(), out);
+    return static_cast<int>(all.size());
+}
+
 }  // extern "C"

@@ -177,6 +177,15 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
                              const uint16_t* depth_mm, int num_classes, const uint8_t* ignore,
                              int subsample_count, int* seed_counter, int capacity,
                              orc_sample* out);
+/* The definition of the project's device classUniform sampler (not a reference algorithm): every
+ * eligible pixel i (label not ignored, depth > 0; i = image * H * W + y * W + x) gets the key
+ * Philox4x32-10(key = (s, 0x53414D50), counter = (i, 0, 0, 0)) word 0, s = the reference
+ * sampler's randomSeed draw; each class keeps its quota of smallest (key, i); samples ordered by
+ * (image, label, y/10, x/10, y, x). Returns the count, -1 if a class has too few pixels. */
+int orc_sample_class_uniform_keys(int n, int width, int height, const uint8_t* labels,
+                                  const uint16_t* depth_mm, int num_classes, const uint8_t* ignore,
+                                  int subsample_count, int* seed_counter, int capacity,
+                                  orc_sample* out);
 
 #ifdef __cplusplus
 }

@@ -264,6 +264,22 @@ def predict(ds, image, trees, normalized, num_classes, threads=1):
     return probs, labels
 
 
+def sample_class_uniform_keys(labels, depth_mm, num_classes, ignore, subsample_count, seed_counter):
+    """The device sampler's definition (keys per pixel); same calling convention as below."""
+    labels = np.ascontiguousarray(labels, dtype=np.uint8)
+    depth_mm = np.ascontiguousarray(depth_mm, dtype=np.uint16)
+    ignore = np.ascontiguousarray(ignore, dtype=np.uint8)
+    n, h, w = labels.shape
+    cap = n * h * w
+    out = np.empty(cap, SAMPLE_DTYPE)
+    sc = ctypes.c_int(seed_counter)
+    rc = lib().orc_sample_class_uniform_keys(n, w, h, _p(labels), _p(depth_mm), num_classes, _p(ignore),
+                                             subsample_count, ctypes.byref(sc), cap, _p(out))
+    if rc < 0:
+        return rc, None, sc.value
+    return rc, out[:rc].copy(), sc.value
+
+
 def sample_class_uniform(labels, depth_mm, num_classes, ignore, subsample_count, seed_counter):
     labels = np.ascontiguousarray(labels, dtype=np.uint8)
     depth_mm = np.ascontiguousarray(depth_mm, dtype=np.uint16)

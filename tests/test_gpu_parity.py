@@ -388,6 +388,41 @@ def test_predict_graph_equals_host_path(ctx, forest_and_oracle):
         g.close()
 
 
+def test_device_sampler_matches_oracle(ctx):
+    rgb, depth, labels = H.frames(seed=8, n=3, w=80, h=60, cells=10, classes=6)
+    ign = np.zeros(6, np.uint8)
+    ign[0] = 1
+    cfg = train_cfg(samples_per_image=300, sampler=1)
+    s, prior, counter = cf.sample_tree_pixels(labels, depth, 6, cfg, 2, 77, ignored=ign, ctx=ctx)
+    rc, o, ocounter = orc.sample_class_uniform_keys(labels, depth, 6, ign, 300 // 2, 77)
+    assert rc == len(s) == 5 * int(np.ceil(3 * 150 / 5))
+    assert counter == ocounter
+    for k in ("x", "y", "image", "label", "flip"):
+        np.testing.assert_array_equal(s[k], o[k], err_msg=k)
+    np.testing.assert_array_equal(s["depth"].view(np.uint32), o["depth"].view(np.uint32))
+    np.testing.assert_array_equal(prior, np.bincount(labels.ravel(), minlength=6))
+    assert (s["label"] != 0).all()
+    # a class with too few eligible pixels is an error, as in the reference
+    with pytest.raises(cf.CurfilError):
+        cf.sample_tree_pixels(labels, depth, 6, train_cfg(samples_per_image=60000, sampler=1), 1, 77, ctx=ctx)
+
+
+def test_forest_train_device_sampler_matches_oracle(ctx):
+    rgb, depth, labels = H.frames(seed=6, n=3, w=80, h=60, cells=10, classes=6)
+    cfg = train_cfg(random_seed=4711, samples_per_image=120, max_depth=7, sampler=1)
+    trees = cf.train_forest(ctx, rgb, depth, labels, 6, cfg, num_trees=2)
+    ods = orc.integral(rgb, depth)
+    SEED = int(orc.sampler_draws(4711, 0, 0xFFFE, 1)[0])
+    for t, tree in enumerate(trees):
+        rc, s, counter = orc.sample_class_uniform_keys(labels, depth, 6, np.zeros(6, np.uint8), 120 // 2, SEED + t)
+        assert rc > 0
+        rc, ot, _ = orc.train_tree(ods, s, 6, 120, 10, 7, 4, 40, 10, counter, threads=4)
+        assert rc == 0
+        g = tree.arrays()
+        o = H.oracle_tree_dict(ot)
+        H.compare_trees(g, o, oracle_scores_ok=lambda i: abs(g["score"][i] - o["score"][i]) <= 1e-6 * o["score"][i])
+
+
 def test_forest_train_end_to_end_matches_oracle(ctx):
     """RandomForestImage::train on raw frames (sampling on the host) vs oracle sampling + training."""
     rgb, depth, labels = H.frames(seed=5, n=3, w=80, h=60, cells=10, classes=6)
