@@ -8,9 +8,12 @@ Workload (the plain-method full-size configuration): 200 seeded synthetic RGB-D 
 
 A step trains the forest's trees level-batched from their sample lists on the resident dataset
 (integral images 1.2 GB, larger than L2). Metric: feature evaluations per second (one evaluation =
-one (sample, candidate feature) response compared against all thresholds and binned).
-`e2e` trains through cf_forest_train from host frames (upload, integral images, host sampling,
-training, tree download). Prediction of 50 frames with the trained forest is reported beside it.
+one (sample, candidate feature) response compared against all thresholds and binned). The split
+search's launch shape is chosen by the autotuner before timing.
+Reported beside it: `e2e` (cf_forest_train from host frames: upload, integral images, device
+sampling, training, tree download; also with the reference's host sampler), the plain per-node form
+on the same tree (identity checked), the CPU oracle, and prediction with a 10-tree forest on 64
+frames (batched, plain per-image form, CUDA-graph replay from host frames, Poisson serving).
 Under torchrun every rank trains its own trees (trees are independent; no collective on the data path).
 """
 import argparse
