@@ -291,8 +291,44 @@ def predict_section(ctx, stream, ds, trees, local, serve_seconds):
     g.close()
     if serve_seconds > 0:
         out["serving"] = serve(forest, serve_seconds)
+    out["refiner"] = refiner_section(ctx, stream, ds, forest, local)
     forest.close()
     return out
+
+
+def refiner_section(ctx, stream, ds, forest, local):
+    """The learned part: the refinement network trained on 32 dataset frames' labels, pixel accuracy
+    of forest and forest + network on 8 held-out frames of the same generator."""
+    import torch
+    import curfil_b200 as cf
+    n_train, n_test = min(32, ds.n), 8
+    _, _, labels = cf.synthetic_frames(W["seed"], n_train, W["width"], W["height"], W["cells"], W["classes"])
+    # held out: the frames after the dataset's in the same seeded sequence (same class appearance)
+    rgb_t, depth_t, labels_t = cf.synthetic_frames(W["seed"], n_test, W["width"], W["height"], W["cells"],
+                                                   W["classes"], first=ds.n)
+    test = cf.Dataset.from_raw(ctx, rgb_t, depth_t)
+    r = cf.Refiner(ctx, W["classes"], hidden=64, epochs=8, batch=4096, pixels_per_image=20000, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = r.train(forest, ds, 0, n_train, labels)
+    train_s = time.perf_counter() - t0
+    lab = torch.empty((n_test, W["height"], W["width"]), dtype=torch.uint8, device=local)
+    forest.predict_dataset(test, 0, n_test, 0, lab.data_ptr())
+    torch.cuda.synchronize()
+    base = float((lab.cpu().numpy() == labels_t).mean())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r.predict(forest, test, 0, n_test, 0, lab.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    refined = float((lab.cpu().numpy() == labels_t).mean())
+    px = n_test * W["width"] * W["height"]
+    r.close()
+    test.close()
+    return {"train_frames": n_train, "train_pixels": n_train * 20000, "epochs": 8, "train_s": train_s,
+            "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "heldout_frames": n_test, "forest_pixel_accuracy": base, "refined_pixel_accuracy": refined,
+            "refined_predict_mpx_per_s": px / (e0.elapsed_time(e1) / 1e3) / 1e6}
 
 
 def serve(forest, seconds):

@@ -609,6 +609,83 @@ class PredictGraph:
             pass
 
 
+class RefinerConfig(ctypes.Structure):
+    _fields_ = [("hidden", ctypes.c_int32), ("radius1", ctypes.c_int32), ("radius2", ctypes.c_int32),
+                ("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("pixels_per_image", ctypes.c_int32),
+                ("learning_rate", ctypes.c_float), ("seed", ctypes.c_uint32)]
+
+    def __init__(self, **kw):
+        d = dict(hidden=64, radius1=4, radius2=16, epochs=8, batch=4096, pixels_per_image=20000,
+                 learning_rate=3e-3, seed=1)
+        d.update(kw)
+        super().__init__(**d)
+
+
+class Refiner:
+    """cf_refiner: the per-pixel refinement network trained on the forest's output (the learned part)."""
+
+    def __init__(self, ctx, num_classes, **config):
+        self.config = RefinerConfig(**config)
+        h = _vp()
+        _check(lib().cf_refiner_create(ctx.handle, int(num_classes), ctypes.byref(self.config), ctypes.byref(h)))
+        self.handle, self.ctx, self.num_classes = h, ctx, int(num_classes)
+        self.num_features = 3 * self.num_classes + 2
+
+    def train(self, forest, ds, first, count, labels, ignored=None):
+        """Returns the mean training loss of every epoch."""
+        labels = np.ascontiguousarray(labels, np.uint8)
+        ign = None if ignored is None else np.ascontiguousarray(ignored, np.uint8)
+        losses = np.zeros(max(1, self.config.epochs), np.float32)
+        _check(lib().cf_refiner_train(self.handle, forest.handle, ds.handle, int(first), int(count), _p(labels),
+                                      _p(ign), _p(losses)))
+        return losses[:self.config.epochs]
+
+    def predict(self, forest, ds, first, count, probs_ptr, labels_ptr):
+        """Device pointers (ints) for the outputs; either may be 0."""
+        _check(lib().cf_refiner_predict(self.handle, forest.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
+                                        _vp(labels_ptr)))
+
+    def params(self, new=None):
+        n = _i32()
+        _check(lib().cf_refiner_params(self.handle, _vp(0), _vp(0), ctypes.byref(n)))
+        if new is not None:
+            new = np.ascontiguousarray(new, np.float32)
+            if new.size != n.value:
+                raise ValueError("expected %d parameters" % n.value)
+            _check(lib().cf_refiner_params(self.handle, _vp(0), _p(new), ctypes.byref(n)))
+        out = np.empty(n.value, np.float32)
+        _check(lib().cf_refiner_params(self.handle, _p(out), _vp(0), ctypes.byref(n)))
+        return out
+
+    def loss_grad(self, features, labels):
+        features = np.ascontiguousarray(features, np.float32)
+        labels = np.ascontiguousarray(labels, np.uint8)
+        n = _i32()
+        _check(lib().cf_refiner_params(self.handle, _vp(0), _vp(0), ctypes.byref(n)))
+        grad = np.empty(n.value, np.float32)
+        loss = ctypes.c_double()
+        _check(lib().cf_refiner_loss_grad(self.handle, len(labels), _p(features), _p(labels), _p(grad),
+                                          ctypes.byref(loss)))
+        return loss.value, grad
+
+    def features(self, forest, ds, frame, xy):
+        xy = np.ascontiguousarray(xy, np.int32)
+        out = np.empty((len(xy), self.num_features), np.float32)
+        _check(lib().cf_refiner_features(self.handle, forest.handle, ds.handle, int(frame), len(xy), _p(xy), _p(out)))
+        return out
+
+    def close(self):
+        if self.handle:
+            _check(lib().cf_refiner_destroy(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """cf_server: continuous-batching dense prediction on a resident forest."""
 
@@ -655,11 +732,12 @@ class Server:
             pass
 
 
-def synthetic_frames(seed, num_images, width, height, num_cells, num_classes, void_class=-1):
-    """Seeded Voronoi RGB-D scenes: (rgb uint8 [n][H][W][3], depth uint16 [n][H][W], labels uint8 [n][H][W])."""
+def synthetic_frames(seed, num_images, width, height, num_cells, num_classes, void_class=-1, first=0):
+    """Seeded Voronoi RGB-D scenes: (rgb uint8 [n][H][W][3], depth uint16 [n][H][W], labels uint8 [n][H][W]),
+    frames first .. first + n - 1 of the seed's sequence."""
     rgb = np.empty((num_images, height, width, 3), np.uint8)
     depth = np.empty((num_images, height, width), np.uint16)
     labels = np.empty((num_images, height, width), np.uint8)
-    _check(lib().cf_synthetic_frames(ctypes.c_uint64(seed), num_images, width, height, num_cells, num_classes,
-                                     void_class, _p(rgb), _p(depth), _p(labels)))
+    _check(lib().cf_synthetic_frames_from(ctypes.c_uint64(seed), int(first), num_images, width, height, num_cells,
+                                          num_classes, void_class, _p(rgb), _p(depth), _p(labels)))
     return rgb, depth, labels

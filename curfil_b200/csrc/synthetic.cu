@@ -88,8 +88,16 @@ void make_frame(uint64_t seed, int img, int W, int H, int K, int C, int void_cla
 extern "C" cf_status cf_synthetic_frames(uint64_t seed, int num_images, int width, int height, int num_cells,
                                          int num_classes, int void_class, uint8_t* rgb, uint16_t* depth_mm,
                                          uint8_t* labels) {
+    return cf_synthetic_frames_from(seed, 0, num_images, width, height, num_cells, num_classes, void_class, rgb,
+                                    depth_mm, labels);
+}
+
+extern "C" cf_status cf_synthetic_frames_from(uint64_t seed, int first_index, int num_images, int width, int height,
+                                              int num_cells, int num_classes, int void_class, uint8_t* rgb,
+                                              uint16_t* depth_mm, uint8_t* labels) {
     return cf::guard([&] {
         CF_REQUIRE(rgb && depth_mm && labels, "cf_synthetic_frames: NULL argument");
+        CF_REQUIRE(first_index >= 0, "cf_synthetic_frames: negative first frame index");
         CF_REQUIRE(num_images >= 1 && width >= 1 && height >= 1 && num_cells >= 1, "cf_synthetic_frames: empty");
         CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_synthetic_frames: classes must be in [1, 256]");
         // class appearance shared by all frames
@@ -106,8 +114,8 @@ extern "C" cf_status cf_synthetic_frames(uint64_t seed, int num_images, int widt
         for (unsigned t = 0; t < nt; t++) {
             pool.emplace_back([&, t] {
                 for (int i = static_cast<int>(t); i < num_images; i += static_cast<int>(nt))
-                    make_frame(seed, i, width, height, num_cells, num_classes, void_class, cls_rgb, cls_depth,
-                               rgb + plane * 3 * i, depth_mm + plane * i, labels + plane * i);
+                    make_frame(seed, first_index + i, width, height, num_cells, num_classes, void_class, cls_rgb,
+                               cls_depth, rgb + plane * 3 * i, depth_mm + plane * i, labels + plane * i);
             });
         }
         for (auto& th : pool) th.join();

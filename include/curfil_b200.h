@@ -351,6 +351,44 @@ cf_status cf_server_counters(cf_server* server, int64_t* submitted, int64_t* com
                              int64_t* batches);
 
 /* ---------------------------------------------------------------------------------------------
+ * The learned part: a per-pixel refinement network on the forest's output (project extension; the
+ * reference has no learned component, its nearest hook is the disabled leaf-histogram refinement,
+ * random_forest_image.cpp:184-255). Input per pixel (D = 3C + 2): the forest's class probabilities,
+ * their means over (2 radius1 + 1)^2 and (2 radius2 + 1)^2 boxes, depth in metres / 5 and a depth-valid
+ * flag; one hidden ReLU layer; softmax cross-entropy; Adam. Parameters (float): W1 [hidden][D],
+ * b1 [hidden], W2 [C][hidden], b2 [C].
+ * ------------------------------------------------------------------------------------------- */
+typedef struct cf_refiner cf_refiner;
+typedef struct cf_refiner_config {
+    int32_t hidden;             /* hidden units, 1..128 */
+    int32_t radius1, radius2;   /* context box radii */
+    int32_t epochs;
+    int32_t batch;              /* pixels per Adam step */
+    int32_t pixels_per_image;   /* training pixels drawn per frame, uniform over labelled pixels */
+    float learning_rate;
+    uint32_t seed;              /* initialisation, pixel draws and shuffling */
+} cf_refiner_config;
+cf_status cf_refiner_create(cf_context* ctx, int num_classes, const cf_refiner_config* config, cf_refiner** out);
+cf_status cf_refiner_destroy(cf_refiner* refiner);
+/* Trains on dataset frames [first, first + count) with host labels uint8 [count][H][W] (ignored[C]
+ * marks classes left out, may be NULL); loss_per_epoch[epochs] receives the mean training loss. */
+cf_status cf_refiner_train(cf_refiner* refiner, cf_forest* forest, cf_dataset* ds, int first, int count,
+                           const uint8_t* labels, const uint8_t* ignored, float* loss_per_epoch);
+/* Refined probabilities float [count][C][H][W] and labels uint8 [count][H][W], DEVICE pointers
+ * (either may be NULL). */
+cf_status cf_refiner_predict(cf_refiner* refiner, cf_forest* forest, cf_dataset* ds, int first, int count,
+                             float* probabilities, uint8_t* labels);
+/* Read (get) and/or replace (set, resets the optimiser) the num_params parameters; host pointers. */
+cf_status cf_refiner_params(cf_refiner* refiner, float* get, const float* set, int* num_params);
+/* Mean loss and its gradient over n given rows (features float [n][D], labels uint8 [n]), computed by
+ * the training kernels; host pointers. */
+cf_status cf_refiner_loss_grad(cf_refiner* refiner, int n, const float* features, const uint8_t* labels,
+                               float* grad, double* loss);
+/* The input rows of n pixels (xy int32 [n][2]) of one dataset frame; out float [n][D], host. */
+cf_status cf_refiner_features(cf_refiner* refiner, cf_forest* forest, cf_dataset* ds, int frame, int n,
+                              const int32_t* xy, float* out);
+
+/* ---------------------------------------------------------------------------------------------
  * Tree files: gzip-compressed JSON (RandomTreeExport::writeJSON export.cpp:292-313,
  * RandomTreeImport::readJSON import.cpp:175-266)
  * ------------------------------------------------------------------------------------------- */
@@ -365,6 +403,11 @@ cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t*
 cf_status cf_synthetic_frames(uint64_t seed, int num_images, int width, int height, int num_cells,
                               int num_classes, int void_class, uint8_t* rgb, uint16_t* depth_mm,
                               uint8_t* labels);
+/* Frames first_index .. first_index + num_images - 1 of the same seeded sequence (frames are
+ * independent given (seed, index); the class appearance depends on the seed only). */
+cf_status cf_synthetic_frames_from(uint64_t seed, int first_index, int num_images, int width, int height,
+                                   int num_cells, int num_classes, int void_class, uint8_t* rgb,
+                                   uint16_t* depth_mm, uint8_t* labels);
 
 #ifdef __cplusplus
 }

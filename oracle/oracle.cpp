@@ -819,6 +819,57 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
     return static_cast<int>(all.size());
 }
 
+/* Mean softmax cross-entropy of the refinement network and its gradient, in double (the CPU
+ * reference for curfil_b200's training kernels). params float: W1 [H][D], b1 [H], W2 [C][H], b2 [C]. */
+void orc_mlp_loss_grad(int n, int D, int H, int C, const float* params, const float* X, const uint8_t* Y,
+                       double* grad, double* loss) {
+    const float* W1 = params;
+    const float* b1 = W1 + static_cast<size_t>(H) * D;
+    const float* W2 = b1 + H;
+    const float* b2 = W2 + static_cast<size_t>(C) * H;
+    const size_t P = static_cast<size_t>(H) * D + H + static_cast<size_t>(C) * H + C;
+    std::fill(grad, grad + P, 0.0);
+    double* gW1 = grad;
+    double* gb1 = gW1 + static_cast<size_t>(H) * D;
+    double* gW2 = gb1 + H;
+    double* gb2 = gW2 + static_cast<size_t>(C) * H;
+    double total = 0;
+    std::vector<double> h(H), z(C), dz(C), g(H);
+    for (int r = 0; r < n; r++) {
+        const float* x = X + static_cast<size_t>(r) * D;
+        for (int j = 0; j < H; j++) {
+            double a = b1[j];
+            for (int k = 0; k < D; k++) a += static_cast<double>(W1[static_cast<size_t>(j) * D + k]) * x[k];
+            h[j] = a > 0 ? a : 0;
+        }
+        double m = -std::numeric_limits<double>::infinity();
+        for (int c = 0; c < C; c++) {
+            double a = b2[c];
+            for (int j = 0; j < H; j++) a += static_cast<double>(W2[static_cast<size_t>(c) * H + j]) * h[j];
+            z[c] = a;
+            m = std::max(m, a);
+        }
+        double s = 0;
+        for (int c = 0; c < C; c++) s += std::exp(z[c] - m);
+        total += std::log(s) + m - z[Y[r]];
+        for (int c = 0; c < C; c++) dz[c] = (std::exp(z[c] - m) / s - (c == Y[r] ? 1.0 : 0.0)) / n;
+        for (int j = 0; j < H; j++) {
+            double a = 0;
+            for (int c = 0; c < C; c++) a += static_cast<double>(W2[static_cast<size_t>(c) * H + j]) * dz[c];
+            g[j] = h[j] > 0 ? a : 0;
+        }
+        for (int c = 0; c < C; c++) {
+            gb2[c] += dz[c];
+            for (int j = 0; j < H; j++) gW2[static_cast<size_t>(c) * H + j] += dz[c] * h[j];
+        }
+        for (int j = 0; j < H; j++) {
+            gb1[j] += g[j];
+            for (int k = 0; k < D; k++) gW1[static_cast<size_t>(j) * D + k] += g[j] * x[k];
+        }
+    }
+    *loss = total / n;
+}
+
 /* The device classUniform sampler's definition (curfil_b200 cf_sample_tree_pixels_device): keys
  * from Philox4x32-10 per eligible pixel, the per-class quota of smallest (key, pixel index), order
  * (image, label, y/10, x/10, y, x). Same seed draws as the reservoir sampler above. */

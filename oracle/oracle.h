@@ -177,6 +177,12 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
                              const uint16_t* depth_mm, int num_classes, const uint8_t* ignore,
                              int subsample_count, int* seed_counter, int capacity,
                              orc_sample* out);
+/* Mean softmax cross-entropy of the project's per-pixel refinement network (h = relu(W1 x + b1),
+ * z = W2 h + b2) over n rows X [n][D] with labels Y [n], and its gradient [P], in double. Not a
+ * reference algorithm: the CPU check of the network's training kernels. */
+void orc_mlp_loss_grad(int n, int D, int H, int C, const float* params, const float* X, const uint8_t* Y,
+                       double* grad, double* loss);
+
 /* The definition of the project's device classUniform sampler (not a reference algorithm): every
  * eligible pixel i (label not ignored, depth > 0; i = image * H * W + y * W + x) gets the key
  * Philox4x32-10(key = (s, 0x53414D50), counter = (i, 0, 0, 0)) word 0, s = the reference

@@ -264,6 +264,18 @@ def predict(ds, image, trees, normalized, num_classes, threads=1):
     return probs, labels
 
 
+def mlp_loss_grad(params, X, Y, hidden, num_classes):
+    """(mean loss, gradient float64 [P]) of the refinement network in double."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.ascontiguousarray(Y, dtype=np.uint8)
+    n, D = X.shape
+    grad = np.empty(params.size, np.float64)
+    loss = ctypes.c_double()
+    lib().orc_mlp_loss_grad(n, D, hidden, num_classes, _p(params), _p(X), _p(Y), _p(grad), ctypes.byref(loss))
+    return loss.value, grad
+
+
 def sample_class_uniform_keys(labels, depth_mm, num_classes, ignore, subsample_count, seed_counter):
     """The device sampler's definition (keys per pixel); same calling convention as below."""
     labels = np.ascontiguousarray(labels, dtype=np.uint8)

@@ -62,6 +62,10 @@ def test_synthetic_frames_deterministic():
     holes = (depth == 0).mean()
     assert 0.05 < holes < 0.15
     assert depth[depth > 0].min() >= 500 and depth.max() <= 5000
+    # frames are independent given (seed, index): a later slice of the sequence equals the tail
+    tail = cf.synthetic_frames(7, 2, 64, 48, 12, 8, first=1)
+    for x, y in zip(a, tail):
+        np.testing.assert_array_equal(x[1:], y)
 
 
 def small_tree(C=3):
