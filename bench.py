@@ -461,7 +461,9 @@ def main():
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
     ds = cf.Dataset.from_raw(ctx, rgb, depth)
-    tree_ids = [rank * W["trees"] + t for t in range(W["trees"])]
+    from curfil_b200 import distributed as cfdist
+    # every rank trains W["trees"] trees of a world * W["trees"] forest (treeId % world == rank)
+    tree_ids = cfdist.tree_ids_for_rank(rank, world, world * W["trees"])
     per_tree = tree_samples(labels, depth, cfg, tree_ids)
     # the split search's launch shape, chosen by the autotuner on this rank's first tree (untimed)
     autotune = None
@@ -507,6 +509,8 @@ def main():
     eval_ms, eval_launches = ctx.kernel_time("level_eval")
     kernel_ms = {k: ctx.kernel_time(k)[0] for k in ("level_eval", "gen_features", "route_flags", "route_scatter",
                                                      "scan", "reduce_candidates", "sort_features")}
+    # the forest of all ranks assembled on every rank (the only exchange; untimed)
+    forest_trees = len(cfdist.gather_forest(trees)) if dist is not None else len(trees)
 
     # algorithmic bytes of the level-batched evaluation: half the candidates are depth features
     bytes_per_eval = (BYTES_DEPTH_EVAL + BYTES_COLOR_EVAL) / 2.0
@@ -594,7 +598,7 @@ def main():
                              "peak_source": peak_kind, "bytes_per_eval": bytes_per_eval,
                              "avg_launch_ms": eval_ms / max(1, eval_launches), "launches": eval_launches},
                 "kernel_ms": kernel_ms,
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "forest_trees": forest_trees,
                 "clocks": clocks.summary(),
                 "predict": predict,
                 "per_node": per_node,
