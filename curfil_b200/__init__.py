@@ -195,12 +195,12 @@ class Dataset:
         self.n, self.width, self.height = int(num_images), int(width), int(height)
 
     @classmethod
-    def from_raw(cls, ctx, rgb, depth_mm):
+    def from_raw(cls, ctx, rgb, depth_mm, fill_depth=False, cie_lab=False):
         rgb = np.ascontiguousarray(rgb, np.uint8)
         depth_mm = np.ascontiguousarray(depth_mm, np.uint16)
         n, h, w = depth_mm.shape
         ds = cls(ctx, n, w, h)
-        ds.upload_raw(rgb, depth_mm)
+        ds.upload_raw(rgb, depth_mm, fill_depth=fill_depth, cie_lab=cie_lab)
         return ds
 
     @classmethod
@@ -212,12 +212,15 @@ class Dataset:
         _check(lib().cf_dataset_upload_integral(ds.handle, 0, n, _p(color), _p(depth)))
         return ds
 
-    def upload_raw(self, rgb, depth_mm, first=0):
+    def upload_raw(self, rgb, depth_mm, first=0, fill_depth=False, cie_lab=False):
+        """Raw frames to integral images; fill_depth / cie_lab as useDepthFilling / useCIELab."""
         if isinstance(rgb, int):
-            _check(lib().cf_dataset_upload_raw(self.handle, first, int(depth_mm[1]), _vp(rgb), _vp(depth_mm[0]), 1))
+            _check(lib().cf_dataset_upload_raw_ex(self.handle, first, int(depth_mm[1]), _vp(rgb), _vp(depth_mm[0]), 1,
+                                                  int(fill_depth), int(cie_lab)))
             return
         n = depth_mm.shape[0]
-        _check(lib().cf_dataset_upload_raw(self.handle, int(first), int(n), _p(rgb), _p(depth_mm), 0))
+        _check(lib().cf_dataset_upload_raw_ex(self.handle, int(first), int(n), _p(rgb), _p(depth_mm), 0,
+                                              int(fill_depth), int(cie_lab)))
 
     def upload_raw_device(self, rgb_ptr, depth_ptr, count, first=0):
         _check(lib().cf_dataset_upload_raw(self.handle, int(first), int(count), _vp(rgb_ptr), _vp(depth_ptr), 1))
@@ -533,6 +536,10 @@ class Forest:
         _check(lib().cf_predict_dataset(self.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
                                         _vp(labels_ptr)))
 
+    def set_preprocessing(self, fill_depth=False, cie_lab=False):
+        """Preprocessing of raw frames before prediction, as the forest was trained."""
+        _check(lib().cf_forest_set_preprocessing(self.handle, int(fill_depth), int(cie_lab)))
+
     def predict_dataset_plain(self, ds, first, count, probs_ptr, labels_ptr):
         """The plain per-image launch form (one launch per tree per image, synchronised)."""
         _check(lib().cf_predict_dataset_plain(self.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
@@ -730,6 +737,51 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def fill_depth(ctx, depth_mm):
+    """RGBDImage::fillDepth on the device; returns a filled copy of uint16 [n][H][W]."""
+    d = np.array(depth_mm, dtype=np.uint16, copy=True, order="C")
+    if d.ndim == 2:
+        d = d[None]
+    n, h, w = d.shape
+    _check(lib().cf_fill_depth(ctx.handle, n, w, h, _p(d), 0))
+    return d
+
+
+def rgb_to_cielab(ctx, rgb):
+    """L*a*b* float32 [n][3][H][W] of uint8 [n][H][W][3], on the device."""
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    n, h, w, _ = rgb.shape
+    out = np.empty((n, 3, h, w), np.float32)
+    _check(lib().cf_rgb_to_cielab(ctx.handle, n, w, h, _p(rgb), _p(out), 0))
+    return out
+
+
+def pixel_accuracy(ctx, prediction_ptr, truth_ptr, count, width, height, num_classes, ignored=None, include_void=True,
+                   confusion=None):
+    """calculatePixelAccuracy over `count` label frames (DEVICE pointers); confusion (uint64 [C][C]) is
+    accumulated when given. Returns the accuracy."""
+    ign = None if ignored is None else np.ascontiguousarray(ignored, np.uint8)
+    if confusion is not None and (confusion.dtype != np.uint64 or confusion.shape != (num_classes, num_classes)):
+        raise ValueError("confusion must be uint64 [C][C]")
+    acc = ctypes.c_double()
+    _check(lib().cf_pixel_accuracy(ctx.handle, int(count), int(width), int(height), _vp(prediction_ptr),
+                                   _vp(truth_ptr), int(num_classes), _p(ign), int(include_void), _p(confusion),
+                                   ctypes.byref(acc)))
+    return acc.value
+
+
+def average_class_accuracy(confusion, ignored=None, include_void=True):
+    """(ConfusionMatrix::averageClassAccuracy, normalised matrix) of a uint64 [C][C] confusion matrix."""
+    confusion = np.ascontiguousarray(confusion, np.uint64)
+    C = confusion.shape[0]
+    ign = None if ignored is None else np.ascontiguousarray(ignored, np.uint8)
+    norm = np.empty((C, C), np.float64)
+    avg = ctypes.c_double()
+    _check(lib().cf_confusion_average_class_accuracy(C, _p(confusion), _p(ign), int(include_void), _p(norm),
+                                                     ctypes.byref(avg)))
+    return avg.value, norm
 
 
 def synthetic_frames(seed, num_images, width, height, num_cells, num_classes, void_class=-1, first=0):

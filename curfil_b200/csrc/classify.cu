@@ -372,6 +372,13 @@ cf_status cf_forest_destroy(cf_forest* forest) {
     });
 }
 
+cf_status cf_forest_set_preprocessing(cf_forest* forest, int fill_depth, int cie_lab) {
+    return guard([&] {
+        CF_REQUIRE(forest, "cf_forest_set_preprocessing: forest is NULL");
+        forest->preprocess = (fill_depth ? kPreFillDepth : 0) | (cie_lab ? kPreCieLab : 0);
+    });
+}
+
 cf_status cf_forest_info(cf_forest* forest, int* num_trees, int* num_classes, int64_t* num_nodes) {
     return guard([&] {
         CF_REQUIRE(forest, "cf_forest_info: forest is NULL");
@@ -423,7 +430,7 @@ cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, c
         CF_CUDA_CHECK(cudaMemcpyAsync(forest->raw_depth.get(), depth_mm, plane * 2 * count, cudaMemcpyHostToDevice,
                                       ctx->stream));
         integrate_frames(ctx, forest->raw_rgb.get(), forest->raw_depth.get(), count, width, height, forest->color.get(),
-                         forest->depth.get());
+                         forest->depth.get(), ctx->stream, forest->preprocess);
         std::vector<FrameDesc>& frames = forest->h_frames;
         frames.resize(count);
         for (int i = 0; i < count; i++) {
@@ -509,7 +516,7 @@ cf_status cf_predict_host_plain(cf_forest* forest, int count, int width, int hei
             CF_CUDA_CHECK(cudaMemcpyAsync(forest->raw_depth.get(), depth_mm + plane * i, plane * 2, cudaMemcpyHostToDevice,
                                           st));
             integrate_frames(ctx, forest->raw_rgb.get(), forest->raw_depth.get(), 1, width, height, forest->color.get(),
-                             forest->depth.get());
+                             forest->depth.get(), ctx->stream, forest->preprocess);
             FrameDesc fr;
             fr.color = forest->color.get();
             fr.depth = forest->depth.get();
@@ -576,7 +583,7 @@ void enqueue_graph_batch(cf_predict_graph* g, int blocks) {
     CF_CUDA_CHECK(cudaMemcpyAsync(g->rgb.get(), g->h_rgb.get(), plane * 3 * n, cudaMemcpyHostToDevice, g->stream));
     CF_CUDA_CHECK(cudaMemcpyAsync(g->depth_mm.get(), g->h_depth.get(), plane * 2 * n, cudaMemcpyHostToDevice, g->stream));
     integrate_frames(ctx, g->rgb.get(), g->depth_mm.get(), g->count, g->width, g->height, g->color.get(), g->dint.get(),
-                     g->stream);
+                     g->stream, g->forest->preprocess);
     classify_frames(ctx, g->forest, g->frames.get(), g->count, blocks, g->stream);
     CF_CUDA_CHECK(cudaMemcpyAsync(g->h_labels.get(), g->labels.get(), plane * n, cudaMemcpyDeviceToHost, g->stream));
     if (g->with_probs)

@@ -28,7 +28,20 @@ void prepare_eval_features(cf_context* ctx, LevelFeatures& lf);
 
 DsView view_of(const cf_dataset* ds);
 
-void integrate_frames(cf_context* ctx, const uint8_t* rgb_dev, const uint16_t* depth_dev, int count, int W, int H,
-                      float* color_out, int2* depth_out, cudaStream_t stream = nullptr);
+// Preprocessing of raw frames (useDepthFilling, useCIELab of TrainingConfiguration).
+constexpr int kPreFillDepth = 1;
+constexpr int kPreCieLab = 2;
+
+// Integral images of `count` raw frames (device pointers). With kPreFillDepth the depth frames are
+// filled IN PLACE first (RGBDImage::fillDepth), so `depth_dev` must then be a buffer the caller owns;
+// with kPreCieLab the colour integral is that of the L*a*b* image.
+void integrate_frames(cf_context* ctx, const uint8_t* rgb_dev, uint16_t* depth_dev, int count, int W, int H,
+                      float* color_out, int2* depth_out, cudaStream_t stream = nullptr, int preprocess = 0);
+
+// preprocess.cu
+void fill_depth_frames(cf_context* ctx, uint16_t* depth, int count, int W, int H, cudaStream_t stream);
+void rgb_to_lab(cf_context* ctx, const uint8_t* rgb, int count, int W, int H, float* lab, cudaStream_t stream);
+void lab_color_integral(cf_context* ctx, const uint8_t* rgb, int count, int W, int H, float* color_out,
+                        cudaStream_t stream);
 
 }  // namespace cf

@@ -44,6 +44,7 @@ struct cf_forest {
     int C = 0;
     int64_t num_nodes = 0;
     int cache_per_tree = 0;          // top nodes of each tree staged in shared memory
+    int preprocess = 0;              // kPreFillDepth | kPreCieLab applied to raw frames before prediction
     std::vector<int> tree_base;      // first node of each tree in `nodes`
     cf::DevArray<cf::PackedNode> nodes;
     cf::DevArray<int> d_tree_base;

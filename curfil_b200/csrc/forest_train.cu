@@ -270,8 +270,17 @@ cf_status cf_forest_train(cf_context* ctx, int num_images, int width, int height
             if (st != CF_OK) fail(st, "cf_forest_train: dataset allocation failed");
         }
         std::unique_ptr<cf_dataset, cf_status (*)(cf_dataset*)> ds(ds_raw, cf_dataset_destroy);
+        // useDepthFilling: the filled depth frames serve the integral images and the sampling
+        std::vector<uint16_t> filled;
+        if (config->use_depth_filling) {
+            filled.assign(depth_mm, depth_mm + static_cast<size_t>(num_images) * width * height);
+            const cf_status st = cf_fill_depth(ctx, num_images, width, height, filled.data(), 0);
+            if (st != CF_OK) fail(st, "cf_forest_train: depth filling failed");
+            depth_mm = filled.data();
+        }
         {
-            const cf_status st = cf_dataset_upload_raw(ds.get(), 0, num_images, rgb, depth_mm, 0);
+            const cf_status st =
+                cf_dataset_upload_raw_ex(ds.get(), 0, num_images, rgb, depth_mm, 0, 0, config->use_cie_lab ? 1 : 0);
             if (st != CF_OK) fail(st, "cf_forest_train: upload failed");
         }
         // RandomForestImage::train: SEED from the configured seed, tree seed SEED + treeId

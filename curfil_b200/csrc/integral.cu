@@ -119,15 +119,17 @@ integral_cols_kernel(int count, int W, int H, uint32_t* __restrict__ color, int2
 }  // namespace
 
 // Integrates `count` raw frames (device pointers) into the given integral buffers.
-void integrate_frames(cf_context* ctx, const uint8_t* rgb_dev, const uint16_t* depth_dev, int count, int W, int H,
-                      float* color_out, int2* depth_out, cudaStream_t stream) {
+void integrate_frames(cf_context* ctx, const uint8_t* rgb_dev, uint16_t* depth_dev, int count, int W, int H,
+                      float* color_out, int2* depth_out, cudaStream_t stream, int preprocess) {
     if (stream == nullptr) stream = ctx->stream;
+    if (preprocess & kPreFillDepth) fill_depth_frames(ctx, depth_dev, count, W, H, stream);
     const long long rows = static_cast<long long>(count) * H;
     launch_on(ctx, stream, "integral_rows", dim3(static_cast<unsigned>((rows + kRowWarps - 1) / kRowWarps)),
            dim3(kRowWarps * 32), 0, integral_rows_kernel, rgb_dev, depth_dev, count, W, H,
            reinterpret_cast<uint32_t*>(color_out), depth_out);
     launch_on(ctx, stream, "integral_cols", dim3((W + 255) / 256, count), dim3(256), 0, integral_cols_kernel, count, W, H,
            reinterpret_cast<uint32_t*>(color_out), depth_out);
+    if (preprocess & kPreCieLab) lab_color_integral(ctx, rgb_dev, count, W, H, color_out, stream);
 }
 
 DsView view_of(const cf_dataset* ds) {
@@ -191,6 +193,11 @@ cf_status cf_dataset_info(cf_dataset* ds, int* num_images, int* width, int* heig
 
 cf_status cf_dataset_upload_raw(cf_dataset* ds, int first, int count, const uint8_t* rgb, const uint16_t* depth_mm,
                                 int device_pointers) {
+    return cf_dataset_upload_raw_ex(ds, first, count, rgb, depth_mm, device_pointers, 0, 0);
+}
+
+cf_status cf_dataset_upload_raw_ex(cf_dataset* ds, int first, int count, const uint8_t* rgb, const uint16_t* depth_mm,
+                                   int device_pointers, int fill_depth, int cie_lab) {
     return cf::guard([&] {
         CF_REQUIRE(ds && rgb && depth_mm, "cf_dataset_upload_raw: NULL argument");
         CF_REQUIRE(first >= 0 && count >= 0 && first + count <= ds->n, "cf_dataset_upload_raw: image range");
@@ -198,26 +205,28 @@ cf_status cf_dataset_upload_raw(cf_dataset* ds, int first, int count, const uint
         cf_context* ctx = ds->ctx;
         cf::make_current(ctx);
         const size_t plane = static_cast<size_t>(ds->width) * ds->height;
-        const uint8_t* rgb_dev = rgb;
-        const uint16_t* depth_dev = depth_mm;
-        if (!device_pointers) {
-            // bounded staging: upload in chunks so large datasets need little extra memory
+        const int pre = (fill_depth ? cf::kPreFillDepth : 0) | (cie_lab ? cf::kPreCieLab : 0);
+        if (!device_pointers || fill_depth) {
+            // bounded staging (the depth frames are filled in place there); chunks keep the extra
+            // memory small for large datasets
+            const cudaMemcpyKind kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
             const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(count, (256u << 20) / (plane * 5))));
             ds->raw_rgb.reserve(plane * 3 * chunk);
             ds->raw_depth.reserve(plane * chunk);
             for (int i = 0; i < count; i += chunk) {
                 const int c = std::min(chunk, count - i);
-                CF_CUDA_CHECK(cudaMemcpyAsync(ds->raw_rgb.get(), rgb + plane * 3 * i, plane * 3 * c,
-                                              cudaMemcpyHostToDevice, ctx->stream));
-                CF_CUDA_CHECK(cudaMemcpyAsync(ds->raw_depth.get(), depth_mm + plane * i, plane * 2 * c,
-                                              cudaMemcpyHostToDevice, ctx->stream));
+                CF_CUDA_CHECK(cudaMemcpyAsync(ds->raw_rgb.get(), rgb + plane * 3 * i, plane * 3 * c, kind, ctx->stream));
+                CF_CUDA_CHECK(cudaMemcpyAsync(ds->raw_depth.get(), depth_mm + plane * i, plane * 2 * c, kind, ctx->stream));
                 cf::integrate_frames(ctx, ds->raw_rgb.get(), ds->raw_depth.get(), c, ds->width, ds->height,
-                                     ds->color.get() + plane * 3 * (first + i), ds->depth.get() + plane * (first + i));
+                                     ds->color.get() + plane * 3 * (first + i), ds->depth.get() + plane * (first + i),
+                                     ctx->stream, pre);
             }
             CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
         } else {
-            cf::integrate_frames(ctx, rgb_dev, depth_dev, count, ds->width, ds->height,
-                                 ds->color.get() + plane * 3 * first, ds->depth.get() + plane * first);
+            // without depth filling the frames are only read
+            cf::integrate_frames(ctx, rgb, const_cast<uint16_t*>(depth_mm), count, ds->width, ds->height,
+                                 ds->color.get() + plane * 3 * first, ds->depth.get() + plane * first, ctx->stream,
+                                 pre);
         }
     });
 }

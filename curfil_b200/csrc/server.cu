@@ -196,7 +196,7 @@ struct cf_server {
             hoff += up(px) + (want_probs ? up(px * 4 * C) : 0);
             CF_CUDA_CHECK(cudaMemcpyAsync(d_rgb, h_rgb, px * 3, cudaMemcpyHostToDevice, slot->stream));
             CF_CUDA_CHECK(cudaMemcpyAsync(d_depth, h_depth, px * 2, cudaMemcpyHostToDevice, slot->stream));
-            integrate_frames(ctx, d_rgb, d_depth, 1, r.W, r.H, d_color, d_int, slot->stream);
+            integrate_frames(ctx, d_rgb, d_depth, 1, r.W, r.H, d_color, d_int, slot->stream, forest->preprocess);
             FrameDesc& fr = slot->h_frames[i];
             fr.color = d_color;
             fr.depth = d_int;

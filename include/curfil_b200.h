@@ -142,6 +142,17 @@ cf_status cf_dataset_destroy(cf_dataset* ds);
  * (0 = missing). `device_pointers` != 0 means both inputs already live in device memory. */
 cf_status cf_dataset_upload_raw(cf_dataset* ds, int first, int count, const uint8_t* rgb,
                                 const uint16_t* depth_mm, int device_pointers);
+/* The same with the reference's image preprocessing: fill_depth = RGBDImage::fillDepth
+ * (image.cpp:279-377, the caller's frames are not modified), cie_lab = colour in CIE L*a*b*
+ * (image.cpp:89-96; the published CIE 1976 formulas with BT.709 primaries and D65 white, as the
+ * reference's Vigra functor implements them for linear RGB). */
+cf_status cf_dataset_upload_raw_ex(cf_dataset* ds, int first, int count, const uint8_t* rgb,
+                                   const uint16_t* depth_mm, int device_pointers, int fill_depth, int cie_lab);
+/* RGBDImage::fillDepth on depth frames uint16 [count][H][W], in place (host or device pointers). */
+cf_status cf_fill_depth(cf_context* ctx, int count, int width, int height, uint16_t* depth_mm, int device_pointers);
+/* The L*a*b* planes float [count][3][H][W] of RGB frames uint8 [count][H][W][3] (before integration). */
+cf_status cf_rgb_to_cielab(cf_context* ctx, int count, int width, int height, const uint8_t* rgb, float* lab,
+                           int device_pointers);
 /* Already-integrated images in the reference layout: colour float [count][3][H][W], depth int32
  * [count][2][H][W] (sum in mm, valid count), e.g. from RGBDImage::getColorImage/getDepthImage. */
 cf_status cf_dataset_upload_integral(cf_dataset* ds, int first, int count, const float* color,
@@ -284,6 +295,9 @@ cf_status cf_forest_create(cf_context* ctx, int num_trees, cf_tree* const* trees
                            double histogram_bias, int use_labels_prior, cf_forest** out);
 cf_status cf_forest_destroy(cf_forest* forest);
 cf_status cf_forest_info(cf_forest* forest, int* num_trees, int* num_classes, int64_t* num_nodes);
+/* Preprocessing of raw frames before prediction (cf_predict_host*, graphs, the server), as the
+ * forest was trained: useDepthFilling and useCIELab of its TrainingConfiguration (default off). */
+cf_status cf_forest_set_preprocessing(cf_forest* forest, int fill_depth, int cie_lab);
 /* Dense prediction of `count` dataset images from `first`: probabilities float [count][C][H][W] and
  * labels uint8 [count][H][W], both DEVICE pointers (either may be NULL). */
 cf_status cf_predict_dataset(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
@@ -396,6 +410,22 @@ cf_status cf_tree_write_json(cf_tree* tree, const cf_train_config* config, const
                              const char* path, int verbose);
 cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t* prior, int prior_capacity,
                             cf_tree** out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Evaluation (predict.cpp:45-207)
+ * ------------------------------------------------------------------------------------------- */
+/* calculatePixelAccuracy over `count` frames: prediction and ground truth uint8 [count][H][W], DEVICE
+ * pointers. Pixels whose true label is marked in ignored[C] (may be NULL) are skipped unless
+ * include_void; accuracy = correct / (all pixels if include_void, else counted pixels). confusion
+ * uint64 [C][C] [label][prediction] (host, may be NULL) is incremented by the counted pixels. */
+cf_status cf_pixel_accuracy(cf_context* ctx, int count, int width, int height, const uint8_t* prediction,
+                            const uint8_t* ground_truth, int num_classes, const uint8_t* ignored, int include_void,
+                            uint64_t* confusion, double* accuracy);
+/* ConfusionMatrix::normalize + averageClassAccuracy: rows normalised by their sums (empty rows stay
+ * 0), the mean of the diagonal over the classes not ignored (all if include_void). normalized
+ * double [C][C] may be NULL. Host only. */
+cf_status cf_confusion_average_class_accuracy(int num_classes, const uint64_t* confusion, const uint8_t* ignored,
+                                              int include_void, double* normalized, double* average);
 
 /* ---------------------------------------------------------------------------------------------
  * Synthetic RGB-D frames (seeded Voronoi scenes) for tests and benchmarks

@@ -819,6 +819,48 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
     return static_cast<int>(all.size());
 }
 
+/* RGBDImage::fillDepth (image.cpp:279-377): passes from the right, left, top and bottom, each
+ * replacing a 0 by its already-processed neighbour. depth uint16 [n][H][W], in place. */
+void orc_fill_depth(int n, int width, int height, uint16_t* depth) {
+    for (int i = 0; i < n; i++) {
+        uint16_t* d = depth + static_cast<size_t>(i) * width * height;
+        for (int y = 0; y < height; y++)
+            for (int x = width - 2; x >= 0; x--)
+                if (!d[y * width + x]) d[y * width + x] = d[y * width + x + 1];
+        for (int y = 0; y < height; y++)
+            for (int x = 1; x < width; x++)
+                if (!d[y * width + x]) d[y * width + x] = d[y * width + x - 1];
+        for (int y = 1; y < height; y++)
+            for (int x = 0; x < width; x++)
+                if (!d[y * width + x]) d[y * width + x] = d[(y - 1) * width + x];
+        for (int y = height - 2; y >= 0; y--)
+            for (int x = 0; x < width; x++)
+                if (!d[y * width + x]) d[y * width + x] = d[(y + 1) * width + x];
+    }
+}
+
+/* CIE 1976 L*a*b* of linear RGB / 255 (BT.709 primaries, D65 white), rounded to float:
+ * rgb uint8 [n][H][W][3] -> lab float [n][3][H][W]. */
+static double lab_f(double t) {
+    return t > 216.0 / 24389.0 ? std::cbrt(t) : t * (841.0 / 108.0) + 4.0 / 29.0;
+}
+
+void orc_rgb_to_lab(int n, int width, int height, const uint8_t* rgb, float* lab) {
+    const size_t plane = static_cast<size_t>(width) * height;
+    for (size_t i = 0; i < n * plane; i++) {
+        const double r = rgb[3 * i] / 255.0, g = rgb[3 * i + 1] / 255.0, b = rgb[3 * i + 2] / 255.0;
+        const double X = 0.412453 * r + 0.357580 * g + 0.180423 * b;
+        const double Y = 0.212671 * r + 0.715160 * g + 0.072169 * b;
+        const double Z = 0.019334 * r + 0.119193 * g + 0.950227 * b;
+        const double fx = lab_f(X / 0.950456), fy = lab_f(Y), fz = lab_f(Z / 1.088754);
+        const size_t img = i / plane, p = i % plane;
+        float* out = lab + img * 3 * plane + p;
+        out[0] = static_cast<float>(116.0 * fy - 16.0);
+        out[plane] = static_cast<float>(500.0 * (fx - fy));
+        out[2 * plane] = static_cast<float>(200.0 * (fy - fz));
+    }
+}
+
 /* Mean softmax cross-entropy of the refinement network and its gradient, in double (the CPU
  * reference for curfil_b200's training kernels). params float: W1 [H][D], b1 [H], W2 [C][H], b2 [C]. */
 void orc_mlp_loss_grad(int n, int D, int H, int C, const float* params, const float* X, const uint8_t* Y,

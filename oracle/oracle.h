@@ -177,6 +177,12 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
                              const uint16_t* depth_mm, int num_classes, const uint8_t* ignore,
                              int subsample_count, int* seed_counter, int capacity,
                              orc_sample* out);
+/* RGBDImage::fillDepth (image.cpp:279-377) on depth uint16 [n][H][W], in place. */
+void orc_fill_depth(int n, int width, int height, uint16_t* depth);
+/* CIE 1976 L*a*b* (linear RGB / 255, BT.709 primaries, D65 white; the published formulas the
+ * reference's Vigra RGB2LabFunctor implements), rounded to float: lab [n][3][H][W]. */
+void orc_rgb_to_lab(int n, int width, int height, const uint8_t* rgb, float* lab);
+
 /* Mean softmax cross-entropy of the project's per-pixel refinement network (h = relu(W1 x + b1),
  * z = W2 h + b2) over n rows X [n][D] with labels Y [n], and its gradient [P], in double. Not a
  * reference algorithm: the CPU check of the network's training kernels. */

@@ -264,6 +264,25 @@ def predict(ds, image, trees, normalized, num_classes, threads=1):
     return probs, labels
 
 
+def fill_depth(depth_mm):
+    """RGBDImage::fillDepth of uint16 [n][H][W] (a filled copy)."""
+    d = np.array(depth_mm, dtype=np.uint16, copy=True, order="C")
+    if d.ndim == 2:
+        d = d[None]
+    n, h, w = d.shape
+    lib().orc_fill_depth(n, w, h, _p(d))
+    return d
+
+
+def rgb_to_lab(rgb):
+    """L*a*b* float32 [n][3][H][W] of uint8 [n][H][W][3]."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    n, h, w, _ = rgb.shape
+    out = np.empty((n, 3, h, w), np.float32)
+    lib().orc_rgb_to_lab(n, w, h, _p(rgb), _p(out))
+    return out
+
+
 def mlp_loss_grad(params, X, Y, hidden, num_classes):
     """(mean loss, gradient float64 [P]) of the refinement network in double."""
     params = np.ascontiguousarray(params, dtype=np.float32)

@@ -113,3 +113,9 @@ PHILOX_KATS = [
     ((0xA4093822, 0x299F31D0, 0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344),
      (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
 ]
+
+# ---- depth filling (image_test.cpp:425-456, testDepthFilling) ------------------------------
+# 200x100 image, every depth invalid except (x=20, y=30) = 1.5 m and (x=30, y=20) = 2.5 m; after
+# RGBDImage::fillDepth every pixel is valid, 2.5 m for y < 30 and 1.5 m from y = 30 on.
+DEPTH_FILL = dict(width=200, height=100, seeds={(20, 30): 1500, (30, 20): 2500}, split_row=30, above=2500,
+                  below=1500)

@@ -1,0 +1,186 @@
+"""Preprocessing (depth filling, CIE L*a*b*) and evaluation helpers on the device vs the oracle.
+
+Bars: depth filling bit-exact (integer work); L*a*b* within one float ulp (the device's double cbrt
+and the host's may differ in the last double bit before the rounding to float); the L*a*b* integral
+within one float ulp plus the double summation-order error; pixel accuracy and the confusion matrix
+exact (integer counts), the class average to 1e-15.
+"""
+import numpy as np
+import pytest
+
+import curfil_b200 as cf
+from oracle import pyoracle as orc
+from tests import helpers as H
+from tests.golden import reference_kats as K
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from curfil_b200 import _build
+    _build.build()
+    c = cf.Context(0)
+    yield c
+    c.close()
+
+
+def holey_depth(rng, n, h, w, frac):
+    d = rng.integers(500, 5001, (n, h, w)).astype(np.uint16)
+    d[rng.random(d.shape) < frac] = 0
+    return d
+
+
+# ------------------------------------------------------------------------------------ depth filling
+def test_fill_depth_kat(ctx):
+    """The reference's own fillDepth test image (image_test.cpp:425-456)."""
+    k = K.DEPTH_FILL
+    d = np.zeros((k["height"], k["width"]), np.uint16)
+    for (x, y), mm in k["seeds"].items():
+        d[y, x] = mm
+    f = cf.fill_depth(ctx, d)[0]
+    assert (f[:k["split_row"]] == k["above"]).all()
+    assert (f[k["split_row"]:] == k["below"]).all()
+
+
+@pytest.mark.parametrize("shape,frac", [((1, 1, 1), 1.0), ((2, 1, 17), 0.6), ((2, 13, 1), 0.6), ((3, 37, 53), 0.3),
+                                        ((2, 37, 53), 0.97), ((1, 480, 640), 0.1)])
+def test_fill_depth_matches_oracle(ctx, shape, frac):
+    rng = np.random.default_rng(sum(shape) + int(frac * 100))
+    d = holey_depth(rng, *shape, frac)
+    d[0, :, :] = 0 if shape[1] * shape[2] < 4 else d[0]
+    got = cf.fill_depth(ctx, d)
+    np.testing.assert_array_equal(got, orc.fill_depth(d))
+    # valid pixels keep their depth
+    np.testing.assert_array_equal(got[d > 0], d[d > 0])
+
+
+def test_fill_depth_all_missing_stays_missing(ctx):
+    d = np.zeros((2, 9, 11), np.uint16)
+    np.testing.assert_array_equal(cf.fill_depth(ctx, d), d)
+
+
+# ------------------------------------------------------------------------------------------ L*a*b*
+def _assert_within_ulps(got, want, ulps=1):
+    """One float ulp, plus 1e-12 absolute for a* and b* near zero, where 500 (fx - fy) cancels terms of
+    size ~100 whose last double bits differ between the device (fused multiply-adds) and the host."""
+    diff = np.abs(got.astype(np.float64) - want.astype(np.float64))
+    bound = ulps * np.spacing(np.abs(want).astype(np.float32)).astype(np.float64) + 1e-12
+    bad = diff > bound
+    assert not bad.any(), (got[bad][:5], want[bad][:5])
+
+
+def test_lab_matches_oracle_all_grey_levels_and_random(ctx):
+    rng = np.random.default_rng(3)
+    grey = np.repeat(np.arange(256, dtype=np.uint8)[:, None], 3, axis=1).reshape(1, 16, 16, 3)
+    rnd = rng.integers(0, 256, (2, 16, 16, 3), dtype=np.uint8)
+    rgb = np.concatenate([grey, rnd])
+    got = cf.rgb_to_cielab(ctx, rgb)
+    want = orc.rgb_to_lab(rgb)
+    _assert_within_ulps(got, want)
+    # white and black
+    assert abs(got[0, 0, 15, 15] - 100.0) < 1e-3 and abs(got[0, 0, 0, 0]) < 1e-6
+
+
+def test_lab_integral_matches_oracle(ctx):
+    rng = np.random.default_rng(11)
+    n, h, w = 2, 61, 83
+    rgb = rng.integers(0, 256, (n, h, w, 3), dtype=np.uint8)
+    depth = holey_depth(rng, n, h, w, 0.2)
+    ds = cf.Dataset.from_raw(ctx, rgb, depth, cie_lab=True)
+    color, dint = ds.download_integral()
+    lab = orc.rgb_to_lab(rgb)
+    for i in range(n):
+        want = orc.integral_float_color(lab[i])
+        absum = np.cumsum(np.cumsum(np.abs(lab[i].astype(np.float64)), axis=1), axis=2)
+        diff = np.abs(color[i].astype(np.float64) - want.astype(np.float64))
+        bound = np.spacing(np.abs(want)).astype(np.float64) + 1e-12 * absum
+        assert (diff <= bound).all()
+    # depth channels untouched by the colour conversion
+    ods = orc.integral(rgb, depth)
+    np.testing.assert_array_equal(dint[:, 1], ods.depth_valid)
+
+
+def test_upload_with_fill_depth_equals_filled_upload(ctx):
+    rng = np.random.default_rng(5)
+    n, h, w = 3, 40, 52
+    rgb = rng.integers(0, 256, (n, h, w, 3), dtype=np.uint8)
+    depth = holey_depth(rng, n, h, w, 0.4)
+    a = cf.Dataset.from_raw(ctx, rgb, depth, fill_depth=True)
+    filled = orc.fill_depth(depth)
+    b = cf.Dataset.from_raw(ctx, rgb, filled)
+    ca, da = a.download_integral()
+    cb, db = b.download_integral()
+    np.testing.assert_array_equal(ca.view(np.uint32), cb.view(np.uint32))
+    np.testing.assert_array_equal(da, db)
+    ods = orc.integral(rgb, filled)
+    np.testing.assert_array_equal(da[:, 1], ods.depth_valid)
+
+
+def test_predict_host_applies_forest_preprocessing(ctx):
+    """A forest marked as trained on filled depth and L*a*b* predicts raw frames like the dataset path
+    over frames uploaded with the same preprocessing."""
+    import torch
+    rgb, depth, labels = H.frames(seed=21, n=3, w=64, h=48, classes=4)
+    depth = depth.copy()
+    depth[np.random.default_rng(1).random(depth.shape) < 0.2] = 0
+    ds = cf.Dataset.from_raw(ctx, rgb, depth, fill_depth=True, cie_lab=True)
+    samples, _ = H.class_uniform_samples(labels, orc.fill_depth(depth), 4, 300)
+    cfg = cf.TrainConfig(feature_count=64, thresholds=10, max_depth=6, min_sample_count=4, box_radius=20,
+                         region_size=6, use_cie_lab=1, use_depth_filling=1)
+    trees = [cf.train_tree(ds, samples, 4, cfg, tree_id=t, seed_counter=5 + t)[0] for t in range(2)]
+    forest = cf.Forest(ctx, trees, prior=np.bincount(labels.ravel(), minlength=4).astype(np.uint32))
+    forest.set_preprocessing(fill_depth=True, cie_lab=True)
+    probs_host, labels_host = forest.predict(rgb, depth)
+    n, h, w = depth.shape
+    probs_dev = torch.empty((n, 4, h, w), dtype=torch.float32, device="cuda")
+    labels_dev = torch.empty((n, h, w), dtype=torch.uint8, device="cuda")
+    forest.predict_dataset(ds, 0, n, probs_dev.data_ptr(), labels_dev.data_ptr())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(labels_host, labels_dev.cpu().numpy())
+    np.testing.assert_array_equal(probs_host, probs_dev.cpu().numpy())
+
+
+# -------------------------------------------------------------------------------------- evaluation
+def _accuracy_restated(pred, truth, C, ignored, include_void):
+    """calculatePixelAccuracy (predict.cpp:148-207) over the given frames."""
+    conf = np.zeros((C, C), np.uint64)
+    keep = np.ones(truth.shape, bool) if include_void or ignored is None else ~np.asarray(ignored, bool)[truth]
+    np.add.at(conf, (truth[keep], pred[keep]), 1)
+    correct = int((pred[keep] == truth[keep]).sum())
+    pixels = truth.size if include_void else int(keep.sum())
+    return correct / pixels, conf
+
+
+@pytest.mark.parametrize("C", [3, 40, 90])
+@pytest.mark.parametrize("include_void", [True, False])
+def test_pixel_accuracy_and_confusion(ctx, C, include_void):
+    import torch
+    rng = np.random.default_rng(C)
+    truth = rng.integers(0, C, (3, 37, 45), dtype=np.uint8)
+    pred = np.where(rng.random(truth.shape) < 0.7, truth, rng.integers(0, C, truth.shape)).astype(np.uint8)
+    ignored = np.zeros(C, np.uint8)
+    ignored[0] = 1
+    want_acc, want_conf = _accuracy_restated(pred, truth, C, ignored, include_void)
+    conf = np.zeros((C, C), np.uint64)
+    conf[0, 0] = 5   # accumulated, not overwritten
+    t_pred = torch.from_numpy(pred).cuda()
+    t_truth = torch.from_numpy(truth).cuda()
+    acc = cf.pixel_accuracy(ctx, t_pred.data_ptr(), t_truth.data_ptr(), 3, 45, 37, C, ignored, include_void, conf)
+    assert acc == pytest.approx(want_acc, rel=0, abs=1e-15)
+    want_conf[0, 0] += 5
+    np.testing.assert_array_equal(conf, want_conf)
+    avg, norm = cf.average_class_accuracy(conf, ignored, include_void)
+    sums = want_conf.astype(np.float64).sum(axis=1, keepdims=True)
+    want_norm = np.where(sums == 0, want_conf.astype(np.float64), want_conf / np.where(sums == 0, 1, sums))
+    np.testing.assert_allclose(norm, want_norm, rtol=1e-15, atol=0)
+    classes = [c for c in range(C) if include_void or not ignored[c]]
+    assert avg == pytest.approx(np.mean([want_norm[c, c] for c in classes]), rel=1e-15)
+
+
+def test_pixel_accuracy_rejects_out_of_range_labels(ctx):
+    import torch
+    truth = torch.full((1, 4, 4), 7, dtype=torch.uint8, device="cuda")
+    pred = torch.zeros((1, 4, 4), dtype=torch.uint8, device="cuda")
+    with pytest.raises(cf.CurfilError):
+        cf.pixel_accuracy(ctx, pred.data_ptr(), truth.data_ptr(), 1, 4, 4, 5)

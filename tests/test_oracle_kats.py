@@ -251,3 +251,34 @@ def test_sampler_range_and_determinism():
     # std::mt19937 default-seed first output is 3499211612 (C++ standard, [rand.predef]);
     # a full-range sampler passes engine words through unchanged
     assert int(orc.sampler_draws(5489, 0, -1, 1)[0]) & 0xFFFFFFFF == 3499211612
+
+
+def test_fill_depth_kat():
+    k = K.DEPTH_FILL
+    d = np.zeros((k["height"], k["width"]), np.uint16)
+    for (x, y), mm in k["seeds"].items():
+        d[y, x] = mm
+    f = orc.fill_depth(d)[0]
+    assert (f[:k["split_row"]] == k["above"]).all()
+    assert (f[k["split_row"]:] == k["below"]).all()
+
+
+def test_fill_depth_leaves_valid_pixels_and_empty_images():
+    rng = np.random.default_rng(4)
+    d = rng.integers(500, 5000, (2, 13, 17)).astype(np.uint16)
+    d[rng.random(d.shape) < 0.4] = 0
+    d[1] = 0                                      # an image without any depth stays empty
+    f = orc.fill_depth(d)
+    assert (f[0][d[0] > 0] == d[0][d[0] > 0]).all()
+    assert (f[0] > 0).all()
+    assert (f[1] == 0).all()
+
+
+def test_lab_reference_white_and_black():
+    rgb = np.array([[[[255, 255, 255], [0, 0, 0], [255, 0, 0]]]], np.uint8)
+    lab = orc.rgb_to_lab(rgb)[0]
+    assert lab[0, 0, 0] == pytest.approx(100.0, abs=1e-4) and abs(lab[1, 0, 0]) < 1e-3 and abs(lab[2, 0, 0]) < 1e-3
+    assert lab[:, 0, 1].tolist() == [0.0, 0.0, 0.0]
+    # pure red (linear RGB): L* = 116 cbrt(0.212671) - 16 = 53.24, a* and b* strongly positive
+    assert lab[0, 0, 2] == pytest.approx(53.2408, abs=1e-3)
+    assert lab[1, 0, 2] > 70 and lab[2, 0, 2] > 60
