@@ -222,6 +222,16 @@ class Dataset:
         _check(lib().cf_dataset_upload_raw_ex(self.handle, int(first), int(n), _p(rgb), _p(depth_mm), 0,
                                               int(fill_depth), int(cie_lab)))
 
+    def upload_raw_padded(self, rgb, depth_mm, first=0, fill_depth=False, cie_lab=False):
+        """Frames smaller than the dataset's, padded as loadImages pads them (RGBDImage::resizeImage)."""
+        rgb = np.ascontiguousarray(rgb, np.uint8)
+        depth_mm = np.ascontiguousarray(depth_mm, np.uint16)
+        if depth_mm.ndim == 2:
+            rgb, depth_mm = rgb[None], depth_mm[None]
+        n, h, w = depth_mm.shape
+        _check(lib().cf_dataset_upload_raw_padded(self.handle, int(first), int(n), int(w), int(h), _p(rgb),
+                                                  _p(depth_mm), 0, int(fill_depth), int(cie_lab)))
+
     def upload_raw_device(self, rgb_ptr, depth_ptr, count, first=0):
         _check(lib().cf_dataset_upload_raw(self.handle, int(first), int(count), _vp(rgb_ptr), _vp(depth_ptr), 1))
 
@@ -737,6 +747,20 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def pad_labels(labels, width, height, padding_label):
+    """LabelImage::resizeImage (image.cpp:763-777): label frames [n][h][w] placed top-left in [n][height][width]
+    frames filled with `padding_label` (getPaddingLabel: the first ignored colour's label, else black's)."""
+    labels = np.asarray(labels, np.uint8)
+    if labels.ndim == 2:
+        labels = labels[None]
+    n, h, w = labels.shape
+    if w > width or h > height:
+        raise ValueError("label frames larger than the padded size")
+    out = np.full((n, height, width), padding_label, np.uint8)
+    out[:, :h, :w] = labels
+    return out
 
 
 def fill_depth(ctx, depth_mm):

@@ -197,7 +197,11 @@ __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, con
                                         (static_cast<uint32_t>(a_ul.x) - static_cast<uint32_t>(a_ll.x)));
         const int s2 = static_cast<int>((static_cast<uint32_t>(b_lr.x) - static_cast<uint32_t>(b_ur.x)) +
                                         (static_cast<uint32_t>(b_ul.x) - static_cast<uint32_t>(b_ll.x)));
-        // 1 <= nv < 2^23 converts exactly through the float bit pattern (no conversion unit)
+        // counts outside [1, 2^23): boxes of more than 2^23 pixels, or negative counts where a box
+        // reaches the zero depth padding of a resized frame (the reference divides by them as they are)
+        if (static_cast<uint32_t>(nv1 - 1) >= 0x7FFFFFu || static_cast<uint32_t>(nv2 - 1) >= 0x7FFFFFu)
+            return bins.exact(exact_depth_response(s1, nv1, s2, nv2));
+        // 1 <= nv < 2^23 (checked above) converts exactly through the float bit pattern (no conversion unit)
         const float n1f = __fsub_rn(__int_as_float(0x4B000000 + nv1), 8388608.0f);
         const float n2f = __fsub_rn(__int_as_float(0x4B000000 + nv2), 8388608.0f);
         const float a = __fdividef(static_cast<float>(s1), n1f) * 0.001f;

@@ -116,6 +116,36 @@ integral_cols_kernel(int count, int W, int H, uint32_t* __restrict__ color, int2
     }
 }
 
+// RGBDImage::resizeImage (image.cpp:450-475) applied to integral images: the w x h integrals go to the
+// top-left corner of the W x H frames, colour NaN and depth {0, 0} everywhere else.
+__global__ void pad_integral_kernel(const float* __restrict__ color_in, const int2* __restrict__ depth_in, int count,
+                                    int w, int h, int W, int H, float* __restrict__ color_out,
+                                    int2* __restrict__ depth_out) {
+    const long long plane = static_cast<long long>(W) * H, small = static_cast<long long>(w) * h;
+    const long long total = plane * count;
+    const float nan = __int_as_float(0x7fc00000);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long img = i / plane;
+        const long long p = i - img * plane;
+        const int y = static_cast<int>(p / W), x = static_cast<int>(p - static_cast<long long>(y) * W);
+        float* c = color_out + img * 3 * plane + p;
+        if (x < w && y < h) {
+            const long long q = img * small + static_cast<long long>(y) * w + x;
+            const float* s = color_in + img * 3 * small + static_cast<long long>(y) * w + x;
+            c[0] = s[0];
+            c[plane] = s[small];
+            c[2 * plane] = s[2 * small];
+            depth_out[i] = depth_in[q];
+        } else {
+            c[0] = nan;
+            c[plane] = nan;
+            c[2 * plane] = nan;
+            depth_out[i] = make_int2(0, 0);
+        }
+    }
+}
+
 }  // namespace
 
 // Integrates `count` raw frames (device pointers) into the given integral buffers.
@@ -228,6 +258,45 @@ cf_status cf_dataset_upload_raw_ex(cf_dataset* ds, int first, int count, const u
                                  ds->color.get() + plane * 3 * first, ds->depth.get() + plane * first, ctx->stream,
                                  pre);
         }
+    });
+}
+
+cf_status cf_dataset_upload_raw_padded(cf_dataset* ds, int first, int count, int width, int height, const uint8_t* rgb,
+                                       const uint16_t* depth_mm, int device_pointers, int fill_depth, int cie_lab) {
+    return cf::guard([&] {
+        CF_REQUIRE(ds && rgb && depth_mm, "cf_dataset_upload_raw_padded: NULL argument");
+        CF_REQUIRE(first >= 0 && count >= 0 && first + count <= ds->n, "cf_dataset_upload_raw_padded: image range");
+        CF_REQUIRE(width >= 1 && height >= 1 && width <= ds->width && height <= ds->height,
+                   "cf_dataset_upload_raw_padded: frames must be at most as large as the dataset's");
+        if (count == 0) return;
+        cf_context* ctx = ds->ctx;
+        cf::make_current(ctx);
+        const size_t small = static_cast<size_t>(width) * height;
+        const size_t plane = static_cast<size_t>(ds->width) * ds->height;
+        const int pre = (fill_depth ? cf::kPreFillDepth : 0) | (cie_lab ? cf::kPreCieLab : 0);
+        const cudaMemcpyKind kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(count, (256u << 20) / (small * 25))));
+        cf::DevArray<uint8_t> raw_rgb;
+        cf::DevArray<uint16_t> raw_depth;
+        cf::DevArray<float> color;
+        cf::DevArray<int2> depth;
+        raw_rgb.reserve(small * 3 * chunk);
+        raw_depth.reserve(small * chunk);
+        color.reserve(small * 3 * chunk);
+        depth.reserve(small * chunk);
+        for (int i = 0; i < count; i += chunk) {
+            const int c = std::min(chunk, count - i);
+            CF_CUDA_CHECK(cudaMemcpyAsync(raw_rgb.get(), rgb + small * 3 * i, small * 3 * c, kind, ctx->stream));
+            CF_CUDA_CHECK(cudaMemcpyAsync(raw_depth.get(), depth_mm + small * i, small * 2 * c, kind, ctx->stream));
+            cf::integrate_frames(ctx, raw_rgb.get(), raw_depth.get(), c, width, height, color.get(), depth.get(),
+                                 ctx->stream, pre);
+            const long long total = static_cast<long long>(plane) * c;
+            const int grid = static_cast<int>(std::min<long long>(ctx->num_sms * 8LL, (total + 255) / 256));
+            cf::launch(ctx, "pad_integral", dim3(grid), dim3(256), 0, cf::pad_integral_kernel, color.get(), depth.get(),
+                       c, width, height, ds->width, ds->height, ds->color.get() + plane * 3 * (first + i),
+                       ds->depth.get() + plane * (first + i));
+        }
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
     });
 }
 

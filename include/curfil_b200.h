@@ -148,6 +148,15 @@ cf_status cf_dataset_upload_raw(cf_dataset* ds, int first, int count, const uint
  * reference's Vigra functor implements them for linear RGB). */
 cf_status cf_dataset_upload_raw_ex(cf_dataset* ds, int first, int count, const uint8_t* rgb,
                                    const uint16_t* depth_mm, int device_pointers, int fill_depth, int cie_lab);
+/* Frames smaller than the dataset's, as loadImages pads them to the largest frame
+ * (LabeledRGBDImage::resizeImage, image.cpp:450-475, 796-800, 904-950): rgb uint8 [count][height][width][3]
+ * and depth_mm [count][height][width] are preprocessed and integrated at their own size, then placed in
+ * the top-left corner of the dataset's frames; the rest of each frame gets colour integral NaN and
+ * depth integral {0, 0}, as RGBDImage::resizeImage leaves it. Labels are padded by the caller
+ * (LabelImage::resizeImage, image.cpp:763-777, with the padding label of getPaddingLabel). */
+cf_status cf_dataset_upload_raw_padded(cf_dataset* ds, int first, int count, int width, int height,
+                                       const uint8_t* rgb, const uint16_t* depth_mm, int device_pointers,
+                                       int fill_depth, int cie_lab);
 /* RGBDImage::fillDepth on depth frames uint16 [count][H][W], in place (host or device pointers). */
 cf_status cf_fill_depth(cf_context* ctx, int count, int width, int height, uint16_t* depth_mm, int device_pointers);
 /* The L*a*b* planes float [count][3][H][W] of RGB frames uint8 [count][H][W][3] (before integration). */

@@ -120,6 +120,19 @@ def integral_float_color(color_planes):
     return out
 
 
+def pad_integral(ds, width, height):
+    """RGBDImage::resizeImage (image.cpp:450-475) on integrated frames: the frames go to the top-left
+    corner of width x height frames; colour NaN and depth sum / valid count 0 elsewhere."""
+    n, _, h, w = ds.color.shape
+    color = np.full((n, 3, height, width), np.nan, np.float32)
+    color[:, :, :h, :w] = ds.color
+    dsum = np.zeros((n, height, width), np.int64)
+    dsum[:, :h, :w] = ds.depth_sum
+    dvalid = np.zeros((n, height, width), np.int32)
+    dvalid[:, :h, :w] = ds.depth_valid
+    return Dataset(color, dsum, dvalid)
+
+
 def pixel_depth(ds, image, x, y):
     return lib().orc_pixel_depth(ds.ref(), image, x, y)
 

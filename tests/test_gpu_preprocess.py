@@ -184,3 +184,93 @@ def test_pixel_accuracy_rejects_out_of_range_labels(ctx):
     pred = torch.zeros((1, 4, 4), dtype=torch.uint8, device="cuda")
     with pytest.raises(cf.CurfilError):
         cf.pixel_accuracy(ctx, pred.data_ptr(), truth.data_ptr(), 1, 4, 4, 5)
+
+
+# --------------------------------------------------------------------------------------------- padding
+def padded_scene(ctx, seed=41, n=3, w=70, h=50, pad_w=96, pad_h=72, classes=40):
+    rgb, depth, labels = H.frames(seed=seed, n=n, w=w, h=h, cells=10, classes=classes)
+    ds = cf.Dataset(ctx, n, pad_w, pad_h)
+    ds.upload_raw_padded(rgb, depth)
+    ods = orc.pad_integral(orc.integral(rgb, depth), pad_w, pad_h)
+    pdepth = np.zeros((n, pad_h, pad_w), np.uint16)
+    pdepth[:, :h, :w] = depth
+    return ds, ods, pdepth, cf.pad_labels(labels, pad_w, pad_h, 0)
+
+
+def test_padded_upload_matches_oracle(ctx):
+    ds, ods, _, labels = padded_scene(ctx)
+    color, dint = ds.download_integral()
+    np.testing.assert_array_equal(np.isnan(color), np.isnan(ods.color))
+    np.testing.assert_array_equal(color.view(np.uint32)[~np.isnan(color)], ods.color.view(np.uint32)[~np.isnan(color)])
+    np.testing.assert_array_equal(dint[:, 0], ods.depth_sum.astype(np.int32))
+    np.testing.assert_array_equal(dint[:, 1], ods.depth_valid)
+    assert (labels[:, 50:, :] == 0).all() and (labels[:, :, 70:] == 0).all()
+    ds.close()
+
+
+def test_padded_upload_with_preprocessing(ctx):
+    rng = np.random.default_rng(2)
+    rgb = rng.integers(0, 256, (2, 30, 40, 3), dtype=np.uint8)
+    depth = holey_depth(rng, 2, 30, 40, 0.3)
+    ds = cf.Dataset(ctx, 2, 64, 48)
+    ds.upload_raw_padded(rgb, depth, fill_depth=True)
+    _, dint = ds.download_integral()
+    ods = orc.pad_integral(orc.integral(rgb, orc.fill_depth(depth)), 64, 48)
+    np.testing.assert_array_equal(dint[:, 1], ods.depth_valid)
+    np.testing.assert_array_equal(dint[:, 0], ods.depth_sum.astype(np.int32))
+    with pytest.raises(cf.CurfilError):
+        ds.upload_raw_padded(np.zeros((1, 50, 40, 3), np.uint8), np.zeros((1, 50, 40), np.uint16))
+    ds.close()
+
+
+@pytest.mark.parametrize("flips", [False, True])
+def test_level_counts_on_padded_frames_bit_exact(ctx, flips):
+    """Boxes that reach the padding see NaN colour and negative depth counts (the reference divides
+    by them); the level-batched kernel's fast paths must count exactly as the oracle does."""
+    ds, ods, pdepth, _ = padded_scene(ctx)
+    rng = np.random.default_rng(7 + flips)
+    sizes = [900, 3, 250, 40]
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    s = H.random_samples(rng, 3, 96, 72, 40, int(offsets[-1]), depth=pdepth, flips=flips)
+    # half of the samples near the edges of the real frame, where boxes straddle the padding
+    k = len(s) // 2
+    s["x"][:k] = rng.integers(50, 70, k)
+    s["y"][:k] = rng.integers(30, 50, k)
+    mm = pdepth[s["image"][:k], s["y"][:k], s["x"][:k]]
+    s["depth"][:k] = np.where(mm > 0, mm.astype(np.float32) / np.float32(1000.0), np.float32(0.0))
+    fe, th = orc.generate_features(ods, s, 123, 96, 12, 60, 15)
+    best, left = cf.level_left_counts(ds, offsets, s, 40, fe, th)
+    for i in range(len(sizes)):
+        sl = s[offsets[i]:offsets[i + 1]]
+        o = orc.histograms(ods, sl.view(orc.SAMPLE_DTYPE), fe, th, 40, threads=4)
+        np.testing.assert_array_equal(left[i], o[:, :, :, 0].transpose(1, 2, 0), err_msg="node %d" % i)
+    ds.close()
+
+
+def test_predict_on_padded_frames_matches_oracle(ctx):
+    import torch
+    C = 6
+    ds, ods, pdepth, labels = padded_scene(ctx, classes=C)
+    ignore = np.zeros(C, np.uint8)
+    ignore[0] = 1   # the padding label is ignored, as getPaddingLabel's colour is
+    samples, _ = H.class_uniform_samples(labels, pdepth, C, 200, ignore=ignore)
+    cfg = cf.TrainConfig(feature_count=128, thresholds=10, max_depth=8, min_sample_count=4, box_radius=40,
+                         region_size=10)
+    tree, _ = cf.train_tree(ds, samples, C, cfg, tree_id=0, seed_counter=9)
+    prior = np.bincount(labels.ravel(), minlength=C).astype(np.uint32)
+    forest = cf.Forest(ctx, [tree], prior=prior)
+    a = tree.arrays()
+    ot = orc.Tree(len(a["left"]), C)
+    ot.left, ot.feature, ot.threshold, ot.histogram = a["left"], a["feature"], a["threshold"], a["histogram"]
+    normalized = np.stack([orc.normalize_histogram(hh, prior, 0.0, True) for hh in a["histogram"]])
+    probs = torch.empty((3, C, 72, 96), dtype=torch.float32, device="cuda")
+    lab = torch.empty((3, 72, 96), dtype=torch.uint8, device="cuda")
+    forest.predict_dataset(ds, 0, 3, probs.data_ptr(), lab.data_ptr())
+    torch.cuda.synchronize()
+    probs, lab = probs.cpu().numpy(), lab.cpu().numpy()
+    for i in range(3):
+        op, ol = orc.predict(ods, i, [ot], [normalized], C, threads=4)
+        assert (lab[i] == ol).mean() >= 0.999
+        np.testing.assert_allclose(probs[i], op, atol=1e-5, rtol=0)
+    forest.close()
+    ds.close()
