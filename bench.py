@@ -510,7 +510,7 @@ def main():
     kernel_ms = {k: ctx.kernel_time(k)[0] for k in ("level_eval", "gen_features", "route_flags", "route_scatter",
                                                      "scan", "reduce_candidates", "sort_features")}
     # the forest of all ranks assembled on every rank (the only exchange; untimed)
-    forest_trees = len(cfdist.gather_forest(trees)) if dist is not None else len(trees)
+    n_forest_trees = len(cfdist.gather_forest(trees)) if dist is not None else len(trees)
 
     # algorithmic bytes of the level-batched evaluation: half the candidates are depth features
     bytes_per_eval = (BYTES_DEPTH_EVAL + BYTES_COLOR_EVAL) / 2.0
@@ -598,7 +598,7 @@ def main():
                              "peak_source": peak_kind, "bytes_per_eval": bytes_per_eval,
                              "avg_launch_ms": eval_ms / max(1, eval_launches), "launches": eval_launches},
                 "kernel_ms": kernel_ms,
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "forest_trees": forest_trees,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "forest_trees": n_forest_trees,
                 "clocks": clocks.summary(),
                 "predict": predict,
                 "per_node": per_node,
