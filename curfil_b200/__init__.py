@@ -546,6 +546,14 @@ class Forest:
         _check(lib().cf_predict_dataset(self.handle, ds.handle, int(first), int(count), _vp(probs_ptr),
                                         _vp(labels_ptr)))
 
+    def predict_dataset_host(self, ds, first, count, probabilities=True):
+        """cf_predict_dataset with host results: (probs float32 [n][C][H][W] or None, labels uint8 [n][H][W])."""
+        h, w = ds.height, ds.width
+        probs = np.empty((count, self.num_classes, h, w), np.float32) if probabilities else None
+        labels = np.empty((count, h, w), np.uint8)
+        _check(lib().cf_predict_dataset_host(self.handle, ds.handle, int(first), int(count), _p(probs), _p(labels)))
+        return probs, labels
+
     def set_preprocessing(self, fill_depth=False, cie_lab=False):
         """Preprocessing of raw frames before prediction, as the forest was trained."""
         _check(lib().cf_forest_set_preprocessing(self.handle, int(fill_depth), int(cie_lab)))
@@ -749,6 +757,27 @@ class Server:
             pass
 
 
+def integrate_planes(ctx, color, depth):
+    """RGBDImage::calculateIntegral of images in the reference layout: colour float32 [n][3][H][W] and
+    depth int32 [n][2][H][W] (mm with 0 invalid, valid flag). Returns the integrated copies."""
+    color = np.array(color, np.float32, copy=True, order="C")
+    depth = np.array(depth, np.int32, copy=True, order="C")
+    n, _, h, w = color.shape
+    if depth.shape != (n, 2, h, w):
+        raise ValueError("depth must be int32 [n][2][H][W]")
+    _check(lib().cf_integrate_planes(ctx.handle, n, w, h, _p(color), _p(depth), _p(color), _p(depth), 0))
+    return color, depth
+
+
+def normalize_histogram(histogram, prior, bias=0.0, use_labels_prior=True):
+    """detail::normalizeHistogram of one histogram with the class prior (host)."""
+    h = np.ascontiguousarray(histogram, np.uint32)
+    p = np.ascontiguousarray(prior, np.uint32)
+    out = np.empty(len(h), np.float64)
+    _check(lib().cf_normalize_histogram(len(h), _p(h), _p(p), ctypes.c_double(bias), int(use_labels_prior), _p(out)))
+    return out
+
+
 def pad_labels(labels, width, height, padding_label):
     """LabelImage::resizeImage (image.cpp:763-777): label frames [n][h][w] placed top-left in [n][height][width]
     frames filled with `padding_label` (getPaddingLabel: the first ignored colour's label, else black's)."""
@@ -792,7 +821,7 @@ def pixel_accuracy(ctx, prediction_ptr, truth_ptr, count, width, height, num_cla
     acc = ctypes.c_double()
     _check(lib().cf_pixel_accuracy(ctx.handle, int(count), int(width), int(height), _vp(prediction_ptr),
                                    _vp(truth_ptr), int(num_classes), _p(ign), int(include_void), _p(confusion),
-                                   ctypes.byref(acc)))
+                                   ctypes.byref(acc), 1))
     return acc.value
 
 

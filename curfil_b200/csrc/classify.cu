@@ -453,6 +453,51 @@ cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, c
     });
 }
 
+cf_status cf_predict_dataset_host(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
+                                  uint8_t* labels) {
+    return guard([&] {
+        CF_REQUIRE(forest && ds, "cf_predict_dataset_host: NULL argument");
+        CF_REQUIRE(first >= 0 && count >= 1 && first + count <= ds->n, "cf_predict_dataset_host: image range");
+        CF_REQUIRE(ds->ctx == forest->ctx, "cf_predict_dataset_host: dataset and forest belong to different contexts");
+        cf_context* ctx = forest->ctx;
+        make_current(ctx);
+        const size_t plane = static_cast<size_t>(ds->width) * ds->height;
+        if (probabilities) forest->probs.reserve(plane * forest->C * count);
+        forest->labels.reserve(plane * count);
+        std::vector<FrameDesc>& frames = forest->h_frames;
+        frames.resize(count);
+        for (int i = 0; i < count; i++) {
+            FrameDesc& fr = frames[i];
+            fr.color = ds->color.get() + (first + i) * plane * 3;
+            fr.depth = ds->depth.get() + (first + i) * plane;
+            fr.probs = probabilities ? forest->probs.get() + plane * forest->C * i : nullptr;
+            fr.labels = forest->labels.get() + plane * i;
+            fr.width = ds->width;
+            fr.height = ds->height;
+            fr.pad = 0;
+        }
+        predict_frames(forest, frames);
+        if (probabilities)
+            CF_CUDA_CHECK(cudaMemcpyAsync(probabilities, forest->probs.get(), sizeof(float) * plane * forest->C * count,
+                                          cudaMemcpyDeviceToHost, ctx->stream));
+        if (labels)
+            CF_CUDA_CHECK(cudaMemcpyAsync(labels, forest->labels.get(), plane * count, cudaMemcpyDeviceToHost, ctx->stream));
+        CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_normalize_histogram(int num_classes, const uint32_t* histogram, const uint32_t* prior,
+                                 double histogram_bias, int use_labels_prior, double* out) {
+    return guard([&] {
+        CF_REQUIRE(histogram && prior && out, "cf_normalize_histogram: NULL argument");
+        CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_normalize_histogram: classes must be in [1, 256]");
+        uint64_t psum = 0;
+        for (int c = 0; c < num_classes; c++) psum += prior[c];
+        CF_REQUIRE(psum > 0, "cf_normalize_histogram: empty class prior");
+        normalize_histogram(num_classes, histogram, prior, histogram_bias, use_labels_prior != 0, out);
+    });
+}
+
 cf_status cf_predict_dataset_plain(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
                                    uint8_t* labels) {
     return guard([&] {

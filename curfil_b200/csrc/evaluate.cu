@@ -59,7 +59,7 @@ extern "C" {
 
 cf_status cf_pixel_accuracy(cf_context* ctx, int count, int width, int height, const uint8_t* prediction,
                             const uint8_t* ground_truth, int num_classes, const uint8_t* ignored, int include_void,
-                            uint64_t* confusion, double* accuracy) {
+                            uint64_t* confusion, double* accuracy, int device_pointers) {
     return guard([&] {
         CF_REQUIRE(ctx && prediction && ground_truth && accuracy, "cf_pixel_accuracy: NULL argument");
         CF_REQUIRE(count >= 1 && width >= 1 && height >= 1, "cf_pixel_accuracy: empty input");
@@ -74,6 +74,14 @@ cf_status cf_pixel_accuracy(cf_context* ctx, int count, int width, int height, c
         DevArray<uint8_t> d_ign;
         DevArray<unsigned long long> d_counts, d_conf;
         DevArray<int> d_bad;
+        DevArray<uint8_t> d_frames;
+        if (!device_pointers) {
+            d_frames.reserve(static_cast<size_t>(2 * n));
+            CF_CUDA_CHECK(cudaMemcpyAsync(d_frames.get(), prediction, n, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(d_frames.get() + n, ground_truth, n, cudaMemcpyHostToDevice, st));
+            prediction = d_frames.get();
+            ground_truth = d_frames.get() + n;
+        }
         d_ign.reserve(C);
         d_counts.reserve(2);
         d_conf.reserve(static_cast<size_t>(C) * C);

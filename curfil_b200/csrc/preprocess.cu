@@ -87,6 +87,32 @@ __global__ void prefix_cols_float_kernel(const double* __restrict__ in, float* _
     }
 }
 
+// 2-D inclusive prefix sums of int32 planes with 32-bit wrap-around (box differences stay exact):
+// rows first (one thread per row), then columns (one thread per column), in place
+__global__ void prefix_rows_int_kernel(int32_t* __restrict__ d, long long rows, int W) {
+    const long long row = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (row >= rows) return;
+    uint32_t* r = reinterpret_cast<uint32_t*>(d) + row * W;
+    uint32_t s = 0;
+    for (int x = 0; x < W; x++) {
+        s += r[x];
+        r[x] = s;
+    }
+}
+
+__global__ void prefix_cols_int_kernel(int32_t* __restrict__ d, long long planes, int W, int H) {
+    const long long col = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (col >= planes * W) return;
+    const long long pl = col / W;
+    const int x = static_cast<int>(col - pl * W);
+    uint32_t* c = reinterpret_cast<uint32_t*>(d) + pl * W * static_cast<long long>(H) + x;
+    uint32_t s = 0;
+    for (int y = 0; y < H; y++) {
+        s += c[static_cast<long long>(y) * W];
+        c[static_cast<long long>(y) * W] = s;
+    }
+}
+
 }  // namespace
 
 void fill_depth_frames(cf_context* ctx, uint16_t* depth, int count, int W, int H, cudaStream_t stream) {
@@ -150,6 +176,58 @@ cf_status cf_fill_depth(cf_context* ctx, int count, int width, int height, uint1
             CF_CUDA_CHECK(cudaMemcpyAsync(depth_mm, d.get(), bytes, cudaMemcpyDeviceToHost, ctx->stream));
         }
         CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+cf_status cf_integrate_planes(cf_context* ctx, int count, int width, int height, const float* color,
+                              const int32_t* depth, float* color_integral, int32_t* depth_integral,
+                              int device_pointers) {
+    return guard([&] {
+        CF_REQUIRE(ctx && color && depth && color_integral && depth_integral, "cf_integrate_planes: NULL argument");
+        CF_REQUIRE(count >= 1 && width >= 1 && height >= 1, "cf_integrate_planes: empty input");
+        make_current(ctx);
+        cudaStream_t st = ctx->stream;
+        const long long plane = static_cast<long long>(width) * height;
+        const long long cplanes = 3LL * count, dplanes = 2LL * count;
+        DevArray<float> d_color;
+        DevArray<double> rows;
+        DevArray<float> d_cout;
+        DevArray<int32_t> d_depth;
+        rows.reserve(static_cast<size_t>(cplanes * plane));
+        const float* c_in = color;
+        float* c_out = color_integral;
+        int32_t* dep = depth_integral;
+        if (!device_pointers) {
+            d_color.reserve(static_cast<size_t>(cplanes * plane));
+            d_cout.reserve(static_cast<size_t>(cplanes * plane));
+            d_depth.reserve(static_cast<size_t>(dplanes * plane));
+            CF_CUDA_CHECK(cudaMemcpyAsync(d_color.get(), color, sizeof(float) * cplanes * plane, cudaMemcpyHostToDevice, st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(d_depth.get(), depth, sizeof(int32_t) * dplanes * plane, cudaMemcpyHostToDevice,
+                                          st));
+            c_in = d_color.get();
+            c_out = d_cout.get();
+            dep = d_depth.get();
+        } else if (depth_integral != depth) {
+            CF_CUDA_CHECK(cudaMemcpyAsync(depth_integral, depth, sizeof(int32_t) * dplanes * plane,
+                                          cudaMemcpyDeviceToDevice, st));
+        }
+        const long long crows = cplanes * height, ccols = cplanes * width;
+        launch(ctx, "integral_planes", dim3(static_cast<unsigned>((crows + 127) / 128)), dim3(128), 0,
+               prefix_rows_double_kernel, c_in, rows.get(), crows, width);
+        launch(ctx, "integral_planes", dim3(static_cast<unsigned>((ccols + 127) / 128)), dim3(128), 0,
+               prefix_cols_float_kernel, rows.get(), c_out, cplanes, width, height);
+        const long long drows = dplanes * height, dcols = dplanes * width;
+        launch(ctx, "integral_planes", dim3(static_cast<unsigned>((drows + 127) / 128)), dim3(128), 0,
+               prefix_rows_int_kernel, dep, drows, width);
+        launch(ctx, "integral_planes", dim3(static_cast<unsigned>((dcols + 127) / 128)), dim3(128), 0,
+               prefix_cols_int_kernel, dep, dplanes, width, height);
+        if (!device_pointers) {
+            CF_CUDA_CHECK(cudaMemcpyAsync(color_integral, c_out, sizeof(float) * cplanes * plane, cudaMemcpyDeviceToHost,
+                                          st));
+            CF_CUDA_CHECK(cudaMemcpyAsync(depth_integral, dep, sizeof(int32_t) * dplanes * plane, cudaMemcpyDeviceToHost,
+                                          st));
+        }
+        CF_CUDA_CHECK(cudaStreamSynchronize(st));
     });
 }
 

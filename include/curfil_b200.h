@@ -157,6 +157,15 @@ cf_status cf_dataset_upload_raw_ex(cf_dataset* ds, int first, int count, const u
 cf_status cf_dataset_upload_raw_padded(cf_dataset* ds, int first, int count, int width, int height,
                                        const uint8_t* rgb, const uint16_t* depth_mm, int device_pointers,
                                        int fill_depth, int cie_lab);
+/* RGBDImage::calculateIntegral (image.cpp:236-277, 531-556) of images in the reference's own layout:
+ * colour float [count][3][H][W] (any float values, as setColor stores them) and depth int32
+ * [count][2][H][W] (depth mm with 0 for invalid, valid 0/1, as setDepth stores them). Colour is summed
+ * in double and rounded to float (identical to the reference's Kahan scan for integer-valued colours;
+ * within the final float rounding otherwise), depth in 32-bit integers that wrap (box differences
+ * stay exact). Outputs have the input layouts; host or device pointers. */
+cf_status cf_integrate_planes(cf_context* ctx, int count, int width, int height, const float* color,
+                              const int32_t* depth, float* color_integral, int32_t* depth_integral,
+                              int device_pointers);
 /* RGBDImage::fillDepth on depth frames uint16 [count][H][W], in place (host or device pointers). */
 cf_status cf_fill_depth(cf_context* ctx, int count, int width, int height, uint16_t* depth_mm, int device_pointers);
 /* The L*a*b* planes float [count][3][H][W] of RGB frames uint8 [count][H][W][3] (before integration). */
@@ -311,6 +320,15 @@ cf_status cf_forest_set_preprocessing(cf_forest* forest, int fill_depth, int cie
  * labels uint8 [count][H][W], both DEVICE pointers (either may be NULL). */
 cf_status cf_predict_dataset(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
                              uint8_t* labels);
+/* cf_predict_dataset with the results copied to HOST buffers (either may be NULL); the
+ * RandomForestImage::predict form for images already integrated (random_forest_image.cpp:258-301). */
+cf_status cf_predict_dataset_host(cf_forest* forest, cf_dataset* ds, int first, int count, float* probabilities,
+                                  uint8_t* labels);
+/* detail::normalizeHistogram (random_tree.cpp:54-104) of one histogram [C] with the class prior [C]:
+ * h'_c = max(0, h_c - bias * sum h), divided by sum h', times prior_c / sum prior when
+ * use_labels_prior. Host only (the reference normalises on the host once per tree). */
+cf_status cf_normalize_histogram(int num_classes, const uint32_t* histogram, const uint32_t* prior,
+                                 double histogram_bias, int use_labels_prior, double* out);
 /* Same from raw host frames, results to host buffers (either may be NULL). */
 cf_status cf_predict_host(cf_forest* forest, int count, int width, int height, const uint8_t* rgb,
                           const uint16_t* depth_mm, float* probabilities, uint8_t* labels);
@@ -424,12 +442,13 @@ cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t*
  * Evaluation (predict.cpp:45-207)
  * ------------------------------------------------------------------------------------------- */
 /* calculatePixelAccuracy over `count` frames: prediction and ground truth uint8 [count][H][W], DEVICE
- * pointers. Pixels whose true label is marked in ignored[C] (may be NULL) are skipped unless
- * include_void; accuracy = correct / (all pixels if include_void, else counted pixels). confusion
- * uint64 [C][C] [label][prediction] (host, may be NULL) is incremented by the counted pixels. */
+ * pointers when device_pointers != 0, else host pointers (copied in). Pixels whose true label is
+ * marked in ignored[C] (may be NULL) are skipped unless include_void; accuracy = correct / (all
+ * pixels if include_void, else counted pixels). confusion uint64 [C][C] [label][prediction] (host,
+ * may be NULL) is incremented by the counted pixels. */
 cf_status cf_pixel_accuracy(cf_context* ctx, int count, int width, int height, const uint8_t* prediction,
                             const uint8_t* ground_truth, int num_classes, const uint8_t* ignored, int include_void,
-                            uint64_t* confusion, double* accuracy);
+                            uint64_t* confusion, double* accuracy, int device_pointers);
 /* ConfusionMatrix::normalize + averageClassAccuracy: rows normalised by their sums (empty rows stay
  * 0), the mean of the diagonal over the classes not ignored (all if include_void). normalized
  * double [C][C] may be NULL. Host only. */

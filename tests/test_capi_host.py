@@ -153,3 +153,20 @@ def test_tree_sampling_matches_oracle():
         np.testing.assert_array_equal(s["depth"].view(np.uint32), o["depth"].view(np.uint32))
         np.testing.assert_array_equal(prior, np.bincount(labels.ravel(), minlength=8))
         assert (s["label"] != 0).all()
+
+
+@pytest.mark.parametrize("kat", range(5))
+def test_normalize_histogram_entry_point_kats(kat):
+    """cf_normalize_histogram (host) against random_tree_test.cpp:46-154 and the oracle."""
+    from oracle import pyoracle as orc
+    from tests.golden import reference_kats as K
+    hist, prior, bias, expected = K.NORMALIZE_KATS[kat]
+    for use_prior in (True, False):
+        got = cf.normalize_histogram(hist, prior, bias, use_prior)
+        np.testing.assert_array_equal(got, orc.normalize_histogram(hist, prior, bias, use_prior))
+    np.testing.assert_allclose(cf.normalize_histogram(hist, prior, bias, True), expected, rtol=1e-15, atol=1e-300)
+
+
+def test_normalize_histogram_rejects_empty_prior():
+    with pytest.raises(cf.CurfilError):
+        cf.normalize_histogram([1, 2], [0, 0])

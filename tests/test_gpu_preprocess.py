@@ -274,3 +274,47 @@ def test_predict_on_padded_frames_matches_oracle(ctx):
         np.testing.assert_allclose(probs[i], op, atol=1e-5, rtol=0)
     forest.close()
     ds.close()
+
+
+# ------------------------------------------------------------------------------ reference-layout integral
+def test_integrate_planes_matches_oracle(ctx):
+    """cf_integrate_planes (RGBDImage::calculateIntegral on setColor/setDepth layouts): integer-valued
+    colours bit-exact, arbitrary floats within one float ulp of the reference's Kahan scan, depth exact."""
+    rng = np.random.default_rng(17)
+    n, h, w = 2, 45, 67
+    rgb = rng.integers(0, 256, (n, h, w, 3), dtype=np.uint8)
+    depth = holey_depth(rng, n, h, w, 0.2)
+    planes = np.ascontiguousarray(rgb.transpose(0, 3, 1, 2).astype(np.float32))
+    dplanes = np.stack([depth.astype(np.int32), (depth > 0).astype(np.int32)], axis=1)
+    color, dint = cf.integrate_planes(ctx, planes, dplanes)
+    ods = orc.integral(rgb, depth)
+    np.testing.assert_array_equal(color.view(np.uint32), ods.color.view(np.uint32))
+    np.testing.assert_array_equal(dint[:, 0], ods.depth_sum.astype(np.int32))
+    np.testing.assert_array_equal(dint[:, 1], ods.depth_valid)
+    floats = (rng.standard_normal((n, 3, h, w)) * 37.3).astype(np.float32)
+    color, _ = cf.integrate_planes(ctx, floats, dplanes)
+    for i in range(n):
+        want = orc.integral_float_color(floats[i])
+        absum = np.cumsum(np.cumsum(np.abs(floats[i].astype(np.float64)), axis=1), axis=2)
+        diff = np.abs(color[i].astype(np.float64) - want.astype(np.float64))
+        assert (diff <= np.spacing(np.abs(want)).astype(np.float64) + 1e-12 * absum).all()
+
+
+def test_predict_dataset_host_equals_device_outputs(ctx):
+    import torch
+    rgb, depth, labels = H.frames(seed=8, n=2, w=64, h=48, classes=5)
+    ds = cf.Dataset.from_raw(ctx, rgb, depth)
+    samples, _ = H.class_uniform_samples(labels, depth, 5, 200)
+    cfg = cf.TrainConfig(feature_count=64, thresholds=10, max_depth=6, min_sample_count=4, box_radius=20,
+                         region_size=6)
+    tree, _ = cf.train_tree(ds, samples, 5, cfg)
+    forest = cf.Forest(ctx, [tree], prior=np.bincount(labels.ravel(), minlength=5).astype(np.uint32))
+    probs_dev = torch.empty((2, 5, 48, 64), dtype=torch.float32, device="cuda")
+    labels_dev = torch.empty((2, 48, 64), dtype=torch.uint8, device="cuda")
+    forest.predict_dataset(ds, 0, 2, probs_dev.data_ptr(), labels_dev.data_ptr())
+    torch.cuda.synchronize()
+    probs, lab = forest.predict_dataset_host(ds, 0, 2)
+    np.testing.assert_array_equal(probs, probs_dev.cpu().numpy())
+    np.testing.assert_array_equal(lab, labels_dev.cpu().numpy())
+    _, lab1 = forest.predict_dataset_host(ds, 1, 1, probabilities=False)
+    np.testing.assert_array_equal(lab1[0], lab[1])
