@@ -65,7 +65,8 @@ class EvalTuning(ctypes.Structure):
     """cf_eval_tuning: launch shape of the level-batched split search (speed only, never results)."""
     _fields_ = [("features_per_tile", ctypes.c_int32), ("bins_budget_words", ctypes.c_int32),
                 ("warp_aggregate", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
-                ("feature_granule", ctypes.c_int32), ("items_per_slot", ctypes.c_float)]
+                ("feature_granule", ctypes.c_int32), ("items_per_slot", ctypes.c_float),
+                ("sample_groups", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

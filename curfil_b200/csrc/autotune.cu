@@ -5,9 +5,9 @@
 // shared-memory tile, node sizes decide how finely a level must be cut into work items) and on the
 // L1/shared-memory split of the GPU. The tuner trains the caller's tree under candidate shapes, takes
 // the device time of the split search (the per-level CUDA events of the trainer), and keeps the
-// fastest by coordinate descent over the histogram budget, the work items per CTA slot, the feature
-// granule and the tile width. Every candidate must produce the identical tree; a difference is an
-// error, never a silent choice.
+// fastest by coordinate descent over the sample mapping and increment aggregation, the histogram
+// budget, the work items per CTA slot, the feature granule and the tile width. Every candidate must
+// produce the identical tree; a difference is an error, never a silent choice.
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -100,6 +100,13 @@ extern "C" cf_status cf_autotune_split_search(cf_dataset* ds, int num_samples, c
                     improved = true;
                 }
             };
+            for (int g = 0; g < 2; g++)
+                for (int agg = 0; agg < 2; agg++) {
+                    cf_eval_tuning c = cur;
+                    c.sample_groups = g;
+                    c.warp_aggregate = agg;
+                    consider(c);
+                }
             for (int v : budgets) {
                 cf_eval_tuning c = cur;
                 c.bins_budget_words = v;

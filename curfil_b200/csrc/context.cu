@@ -225,6 +225,7 @@ cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning) {
                    "cf_context_set_tuning: feature_granule must be in [1, 64]");
         CF_REQUIRE(t.items_per_slot > 0.0f && t.items_per_slot <= 1024.0f,
                    "cf_context_set_tuning: items_per_slot must be in (0, 1024]");
+        CF_REQUIRE(t.sample_groups == 0 || t.sample_groups == 1, "cf_context_set_tuning: sample_groups is 0 or 1");
         std::lock_guard<std::mutex> lock(ctx->mu);
         ctx->tuning = t;
     });

@@ -109,7 +109,7 @@ __device__ __noinline__ double score_from_cum(const uint32_t* cum, int stride, c
     return normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, hc)));
 }
 
-template <bool kAgg, bool kPad32, int kMinBlocks>
+template <bool kAgg, bool kPad32, int kMinBlocks, bool kGrouped>
 __global__ void __launch_bounds__(256, kMinBlocks)
 level_eval_kernel(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -128,7 +128,10 @@ level_eval_kernel(EvalArgs a) {
     __shared__ double s_drop;
 
     const int TP = kPad32 ? kPadThresholds : a.T;
-    const SmemLayout L(a.C, a.T, TP, a.ft_max, a.bins_budget);
+    // threshold row stride in shared memory: with sample groups the lanes of a warp search different
+    // features' rows at the same position, so the rows are skewed by one bank
+    const int TPS = TP + (kGrouped ? 1 : 0);
+    const SmemLayout L(a.C, a.T, TP + 1, a.ft_max, a.bins_budget);
     uint32_t* s_counts = reinterpret_cast<uint32_t*>(smem + L.counts);
     EvalFeat* s_params = reinterpret_cast<EvalFeat*>(smem + L.params);
     float* s_thr = reinterpret_cast<float*>(smem + L.thr);
@@ -201,10 +204,10 @@ level_eval_kernel(EvalArgs a) {
             if (kPad32) {
                 for (int i = tid; i < nf * kPadThresholds; i += blockDim.x) {
                     const int t = i & (kPadThresholds - 1);
-                    s_thr[i] = t < T ? g_thr[(i >> 5) * T + t] : INFINITY;
+                    s_thr[(i >> 5) * TPS + t] = t < T ? g_thr[(i >> 5) * T + t] : INFINITY;
                 }
             } else {
-                for (int i = tid; i < nf * T; i += blockDim.x) s_thr[i] = g_thr[i];
+                for (int i = tid; i < nf * T; i += blockDim.x) s_thr[(i / T) * TPS + i % T] = g_thr[i];
             }
             for (int i = tid; i < nf * T; i += blockDim.x) s_rank[i] = a.ranks[static_cast<long long>(f0) * T + i];
             const int nbins = nf * cp * T1;
@@ -213,7 +216,64 @@ level_eval_kernel(EvalArgs a) {
 
             const int W = a.ds.width, H = a.ds.height;
             const int nthr = blockDim.x;
-            const int n_major = (N / nthr) * nthr;
+            const int n_major = kGrouped ? 0 : (N / nthr) * nthr;
+            if constexpr (kGrouped) {
+                // ---- histogram, sample groups: the lanes of a warp take (sample, feature) pairs of a
+                // few consecutive samples (FL lanes per sample, FL = nf rounded up to a power of two,
+                // at most 32) and the warps of the CTA the next groups. The samples in flight on an SM
+                // are then neighbours in the node's order, close together in the image, and the
+                // corner gathers of their features share L1 lines.
+                const int FL = nf >= 32 ? 32 : (nf <= 1 ? 1 : 1 << (32 - __clz(nf - 1)));
+                const int SPW = 32 / FL;
+                const int fl = lane & (FL - 1);
+                const int js = lane / FL;
+                const int step = static_cast<int>(blockDim.x >> 5) * SPW;
+                if (nf <= 32) {
+                    // every lane keeps one feature for all its samples: parameters in registers
+                    const bool fa = fl < nf;
+                    const int fc = fa ? fl : 0;
+                    const EvalFeat ef = s_params[fc];
+                    const SortedBins<kPad32> sorted{s_thr + fc * TPS, T};
+                    for (int s0 = warp * SPW; s0 < N; s0 += step) {   // trip count uniform in a warp
+                        const int s = s0 + js;
+                        const bool act = fa && s < N;
+                        const Sample smp = a.samples[nd.start + min(s, N - 1)];
+                        const EvalPixel px = make_eval_pixel(a.ds, smp);
+                        const int row = (fc * cp + s_lid[smp.label]) * T1;
+                        const int flip = smp.flip;
+                        const int key1 = act ? row + feature_bin(px, W, H, ef, flip == 1, sorted) : -1;
+                        bin_increment<kAgg>(s_bins, key1);
+                        if (__any_sync(kFull, act && flip == 2)) {
+                            const int key2 = act && flip == 2 ? row + feature_bin(px, W, H, ef, true, sorted) : -1;
+                            bin_increment<kAgg>(s_bins, key2);
+                        }
+                    }
+                } else {
+                    for (int s0 = warp * SPW; s0 < N; s0 += step) {
+                        const int s = s0 + js;
+                        const bool sv = s < N;
+                        const Sample smp = a.samples[nd.start + min(s, N - 1)];
+                        const EvalPixel px = make_eval_pixel(a.ds, smp);
+                        const int lid = s_lid[smp.label];
+                        const int flip = smp.flip;
+                        const bool any_both = __any_sync(kFull, sv && flip == 2);
+                        for (int fb = 0; fb < nf; fb += FL) {
+                            const int f = fb + fl;
+                            const bool act = sv && f < nf;
+                            const int fc = act ? f : 0;
+                            const SortedBins<kPad32> sorted{s_thr + fc * TPS, T};
+                            const int row = (fc * cp + lid) * T1;
+                            const int key1 = act ? row + feature_bin(px, W, H, s_params[fc], flip == 1, sorted) : -1;
+                            bin_increment<kAgg>(s_bins, key1);
+                            if (any_both) {
+                                const int key2 =
+                                    act && flip == 2 ? row + feature_bin(px, W, H, s_params[fc], true, sorted) : -1;
+                                bin_increment<kAgg>(s_bins, key2);
+                            }
+                        }
+                    }
+                }
+            }
             // ---- histogram, sample-major over whole blocks of samples: each thread keeps one sample
             // and walks the tile's features, so the sample's neighbourhood is reused from L1
             for (int s0 = 0; s0 < n_major; s0 += nthr) {
@@ -228,8 +288,8 @@ level_eval_kernel(EvalArgs a) {
                 for (; f + 1 < nf; f += 2) {
                     const EvalFeat& fa = s_params[f];
                     const EvalFeat& fb = s_params[f + 1];
-                    const SortedBins<kPad32> sa{s_thr + f * TP, T};
-                    const SortedBins<kPad32> sb{s_thr + (f + 1) * TP, T};
+                    const SortedBins<kPad32> sa{s_thr + f * TPS, T};
+                    const SortedBins<kPad32> sb{s_thr + (f + 1) * TPS, T};
                     const int row_a = (f * cp + lid) * T1;
                     const int row_b = row_a + cp * T1;
                     const int ka = row_a + feature_bin(px, W, H, fa, flip == 1, sa);
@@ -245,7 +305,7 @@ level_eval_kernel(EvalArgs a) {
                 }
                 if (f < nf) {
                     const EvalFeat& fp = s_params[f];
-                    const SortedBins<kPad32> sorted{s_thr + f * TP, T};
+                    const SortedBins<kPad32> sorted{s_thr + f * TPS, T};
                     const int row = (f * cp + lid) * T1;
                     const int key1 = row + feature_bin(px, W, H, fp, flip == 1, sorted);
                     bin_increment<kAgg>(s_bins, key1);
@@ -258,7 +318,7 @@ level_eval_kernel(EvalArgs a) {
             // ---- the remaining Nt < blockDim samples, pair-major: pairs p = f * Nt + s spread over
             // all threads with a uniform trip count so warps stay converged
             const int Nt = N - n_major;
-            if (Nt > 0) {
+            if (!kGrouped && Nt > 0) {
                 const Sample* tail = a.samples + nd.start + n_major;
                 const long long pairs = static_cast<long long>(nf) * Nt;
                 const int iters = static_cast<int>((pairs + nthr - 1) / nthr);
@@ -272,7 +332,7 @@ level_eval_kernel(EvalArgs a) {
                         const Sample smp = tail[s];
                         const EvalPixel px = make_eval_pixel(a.ds, smp);
                         const EvalFeat& fp = s_params[f];
-                        const SortedBins<kPad32> sorted{s_thr + f * TP, T};
+                        const SortedBins<kPad32> sorted{s_thr + f * TPS, T};
                         const int row = (f * cp + s_lid[smp.label]) * T1;
                         key1 = row + feature_bin(px, W, H, fp, smp.flip == 1, sorted);
                         if (smp.flip == 2) key2 = row + feature_bin(px, W, H, fp, true, sorted);
@@ -564,7 +624,7 @@ __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const 
 SmemLayout level_eval_smem(int C, int T, const EvalTuning& tuning, int* budget) {
     *budget = std::max(tuning.bins_budget_words, C * (T + 1));
     const int TP = T < kPadThresholds ? kPadThresholds : T;
-    return SmemLayout(C, T, TP, tuning.ft_max, *budget);
+    return SmemLayout(C, T, TP + 1, tuning.ft_max, *budget);   // rows skewed by one bank with sample groups
 }
 
 // Shared-memory carveout (percent of the SM's 228 KB) that just holds `ctas` CTAs of `smem` dynamic
@@ -580,15 +640,22 @@ void set_level_eval_smem(K kernel, size_t smem, int ctas) {
     CF_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
 }
 
-template <bool kAgg, bool kPad32>
-void launch_level_eval_t(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm) {
+template <bool kAgg, bool kPad32, bool kGrouped>
+void launch_level_eval_g(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm) {
     if (ctas_per_sm >= 4) {
-        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 4>, smem, ctas_per_sm);
-        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 4>, args);
+        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 4, kGrouped>, smem, ctas_per_sm);
+        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 4, kGrouped>, args);
     } else {
-        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 3>, smem, ctas_per_sm);
-        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 3>, args);
+        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 3, kGrouped>, smem, ctas_per_sm);
+        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 3, kGrouped>, args);
     }
+}
+
+template <bool kAgg, bool kPad32>
+void launch_level_eval_t(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm,
+                         bool grouped) {
+    if (grouped) launch_level_eval_g<kAgg, kPad32, true>(ctx, args, grid, smem, ctas_per_sm);
+    else launch_level_eval_g<kAgg, kPad32, false>(ctx, args, grid, smem, ctas_per_sm);
 }
 
 // The level_eval instance for the tuning and threshold count (T <= 31 takes the padded search).
@@ -599,12 +666,13 @@ void launch_level_eval(cf_context* ctx, const EvalArgs& args, int grid, const Ev
                "split search: classes x thresholds too large for shared memory");
     CF_REQUIRE(args.bins_budget == budget && args.ft_max == tuning.ft_max, "split search: inconsistent tuning");
     const bool pad = args.T < kPadThresholds;
+    const bool g = tuning.sample_groups != 0;
     if (tuning.warp_aggregate) {
-        if (pad) launch_level_eval_t<true, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
-        else launch_level_eval_t<true, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
+        if (pad) launch_level_eval_t<true, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
+        else launch_level_eval_t<true, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
     } else {
-        if (pad) launch_level_eval_t<false, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
-        else launch_level_eval_t<false, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm);
+        if (pad) launch_level_eval_t<false, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
+        else launch_level_eval_t<false, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
     }
 }
 
@@ -623,6 +691,7 @@ EvalTuning EvalTuning::of(cf_context* ctx) {
     e.ctas_per_sm = t.ctas_per_sm;
     e.items_per_slot = t.items_per_slot;
     e.feature_granule = t.feature_granule;
+    e.sample_groups = t.sample_groups;
     return e;
 }
 

@@ -44,6 +44,7 @@ struct EvalTuning {
     int ctas_per_sm = 3;
     double items_per_slot = 64.0; // work items per resident CTA for load balance
     int feature_granule = 8;      // a work item covers a multiple of this many features
+    int sample_groups = 0;        // 1: lanes take (sample, feature) pairs of consecutive samples
 
     static EvalTuning of(cf_context* ctx);
 };

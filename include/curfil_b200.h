@@ -118,12 +118,16 @@ typedef struct cf_eval_tuning {
     int32_t ctas_per_sm;         /* resident CTAs per SM the kernel is compiled for, 1..4 (default 3) */
     int32_t feature_granule;     /* work items cover a multiple of this many features, 1..64 (default 8) */
     float items_per_slot;        /* work items per resident CTA, (0, 1024] (default 64) */
+    int32_t sample_groups;       /* 0: each thread takes one sample through the tile's features; 1: the
+                                    lanes of a warp take (sample, feature) pairs of a few consecutive
+                                    samples (neighbours in the image, so gathers share L1 lines) */
 } cf_eval_tuning;
 cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out);
 cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning);
 /* Project-written autotuner (no reference counterpart): trains the given tree (as cf_train_tree,
  * level-batched) under candidate launch shapes, starting from the context's current one, by
- * coordinate descent over bins_budget_words, items_per_slot, feature_granule and features_per_tile,
+ * coordinate descent over (sample_groups, warp_aggregate), bins_budget_words, items_per_slot,
+ * feature_granule and features_per_tile,
  * timing the split search with the trainer's CUDA events (min over `repeats`). Every candidate must
  * yield the identical tree (else CF_ERR_STATE). The fastest shape is set on the context and returned
  * with its time; `start_ms` is the time of the starting shape, `trials` the shapes measured (either

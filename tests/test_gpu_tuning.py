@@ -16,6 +16,9 @@ TUNINGS = [
     {"bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1, "items_per_slot": 1000.0},
     {"ctas_per_sm": 1, "items_per_slot": 0.5, "feature_granule": 64, "features_per_tile": 64},
     {"ctas_per_sm": 2, "bins_budget_words": 49152, "items_per_slot": 4.0, "feature_granule": 4},
+    {"sample_groups": 1},
+    {"sample_groups": 1, "warp_aggregate": 0, "features_per_tile": 64, "feature_granule": 64},
+    {"sample_groups": 1, "bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1},
 ]
 
 
