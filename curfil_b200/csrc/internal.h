@@ -146,8 +146,9 @@ struct cf_context {
 
     // measured on B200 with 200 frames 640x480, 40 classes, 2000 features x 20 thresholds: a 28 KB
     // histogram leaves ~140 KB of the SM's unified memory to L1 for the integral-image gathers, and
-    // ~64 items per CTA slot keep the last wave of a level short
-    static cf_eval_tuning default_tuning() { return cf_eval_tuning{32, 7168, 1, 3, 8, 64.0f, 0}; }
+    // ~64 items per CTA slot keep the last wave of a level short; sample groups without increment
+    // aggregation were 8 % faster than thread-per-sample with aggregation
+    static cf_eval_tuning default_tuning() { return cf_eval_tuning{32, 7168, 0, 3, 8, 64.0f, 1}; }
     std::mutex mu;
     struct KernelEvents {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;

@@ -29,6 +29,7 @@ namespace cf {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kUnroll = 2;   // samples per lane and step in the sample-group mapping (4 spills and is slower)
 
 template <bool kAgg>
 __device__ __forceinline__ void bin_increment(uint32_t* bins, int key) {
@@ -234,18 +235,34 @@ level_eval_kernel(EvalArgs a) {
                     const int fc = fa ? fl : 0;
                     const EvalFeat ef = s_params[fc];
                     const SortedBins<kPad32> sorted{s_thr + fc * TPS, T};
-                    for (int s0 = warp * SPW; s0 < N; s0 += step) {   // trip count uniform in a warp
-                        const int s = s0 + js;
-                        const bool act = fa && s < N;
-                        const Sample smp = a.samples[nd.start + min(s, N - 1)];
-                        const EvalPixel px = make_eval_pixel(a.ds, smp);
-                        const int row = (fc * cp + s_lid[smp.label]) * T1;
-                        const int flip = smp.flip;
-                        const int key1 = act ? row + feature_bin(px, W, H, ef, flip == 1, sorted) : -1;
-                        bin_increment<kAgg>(s_bins, key1);
-                        if (__any_sync(kFull, act && flip == 2)) {
-                            const int key2 = act && flip == 2 ? row + feature_bin(px, W, H, ef, true, sorted) : -1;
-                            bin_increment<kAgg>(s_bins, key2);
+                    // kUnroll samples per lane and step: their gathers are independent and overlap
+                    for (int s0 = warp * SPW; s0 < N; s0 += kUnroll * step) {   // trip count uniform in a warp
+                        EvalPixel px[kUnroll];
+                        int row[kUnroll], flip[kUnroll], key[kUnroll];
+                        bool act[kUnroll];
+#pragma unroll
+                        for (int u = 0; u < kUnroll; u++) {
+                            const int s = s0 + js + u * step;
+                            act[u] = fa && s < N;
+                            const Sample m = a.samples[nd.start + min(s, N - 1)];
+                            px[u] = make_eval_pixel(a.ds, m);
+                            row[u] = (fc * cp + s_lid[m.label]) * T1;
+                            flip[u] = act[u] ? m.flip : 0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < kUnroll; u++)
+                            key[u] = act[u] ? row[u] + feature_bin(px[u], W, H, ef, flip[u] == 1, sorted) : -1;
+#pragma unroll
+                        for (int u = 0; u < kUnroll; u++) bin_increment<kAgg>(s_bins, key[u]);
+                        bool both = false;
+#pragma unroll
+                        for (int u = 0; u < kUnroll; u++) both = both || flip[u] == 2;
+                        if (__any_sync(kFull, both)) {
+#pragma unroll
+                            for (int u = 0; u < kUnroll; u++)
+                                key[u] = flip[u] == 2 ? row[u] + feature_bin(px[u], W, H, ef, true, sorted) : -1;
+#pragma unroll
+                            for (int u = 0; u < kUnroll; u++) bin_increment<kAgg>(s_bins, key[u]);
                         }
                     }
                 } else {

@@ -114,12 +114,12 @@ cf_status cf_context_device(cf_context* ctx, char* name, size_t name_length, int
 typedef struct cf_eval_tuning {
     int32_t features_per_tile;   /* features per shared-memory tile at most, 2..64 (default 32) */
     int32_t bins_budget_words;   /* histogram words per CTA, 1024..49152 (default 7168) */
-    int32_t warp_aggregate;      /* 1: warp-aggregated shared increments (default), 0: plain atomics */
+    int32_t warp_aggregate;      /* 1: warp-aggregated shared increments, 0: plain atomics (default) */
     int32_t ctas_per_sm;         /* resident CTAs per SM the kernel is compiled for, 1..4 (default 3) */
     int32_t feature_granule;     /* work items cover a multiple of this many features, 1..64 (default 8) */
     float items_per_slot;        /* work items per resident CTA, (0, 1024] (default 64) */
-    int32_t sample_groups;       /* 0: each thread takes one sample through the tile's features; 1: the
-                                    lanes of a warp take (sample, feature) pairs of a few consecutive
+    int32_t sample_groups;       /* 0: each thread takes one sample through the tile's features; 1 (default):
+                                    the lanes of a warp take (sample, feature) pairs of a few consecutive
                                     samples (neighbours in the image, so gathers share L1 lines) */
 } cf_eval_tuning;
 cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out);

@@ -11,14 +11,15 @@ pytestmark = pytest.mark.gpu
 
 TUNINGS = [
     {},
-    {"warp_aggregate": 0},
+    {"warp_aggregate": 1},
+    {"sample_groups": 0},
+    {"sample_groups": 0, "warp_aggregate": 1},
     {"ctas_per_sm": 4, "bins_budget_words": 4096},
     {"bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1, "items_per_slot": 1000.0},
+    {"sample_groups": 0, "bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1},
     {"ctas_per_sm": 1, "items_per_slot": 0.5, "feature_granule": 64, "features_per_tile": 64},
+    {"sample_groups": 0, "ctas_per_sm": 1, "feature_granule": 64, "features_per_tile": 64},
     {"ctas_per_sm": 2, "bins_budget_words": 49152, "items_per_slot": 4.0, "feature_granule": 4},
-    {"sample_groups": 1},
-    {"sample_groups": 1, "warp_aggregate": 0, "features_per_tile": 64, "feature_granule": 64},
-    {"sample_groups": 1, "bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1},
 ]
 
 
@@ -41,7 +42,8 @@ def scene(ctx):
 def test_default_tuning_and_reset(ctx):
     ctx.set_tuning()
     d = ctx.get_tuning().as_dict()
-    assert d["ctas_per_sm"] == 3 and d["warp_aggregate"] == 1 and d["features_per_tile"] == 32
+    assert d["ctas_per_sm"] == 3 and d["warp_aggregate"] == 0 and d["features_per_tile"] == 32
+    assert d["sample_groups"] == 1
     ctx.set_tuning(items_per_slot=2.0)
     assert ctx.get_tuning().items_per_slot == 2.0
     ctx.set_tuning()
