@@ -36,6 +36,10 @@ W = dict(images=200, width=640, height=480, cells=40, classes=40, samples_per_im
          predict_trees=10, seed=2026)
 # serving: Poisson arrivals of mixed frame sizes (weights 1:2:4:1) at these offered rates
 SERVE_RATES = (200, 1000, 4000)
+# cf_server_config of the serving runs: one 640x480 frame already fills the GPU, so small batches cost
+# no throughput and keep a frame from waiting for a long batch (p99 at 1000 frames/s: 12 ms with 2
+# frames per batch, 20 ms with 32)
+SERVE_CONFIG = dict(max_batch_frames=2, pipeline_depth=3)
 SERVE_SIZES = ((160, 120, 1), (320, 240, 2), (640, 480, 4), (1280, 960, 1))
 BYTES_DEPTH_EVAL = 64   # 2 boxes x 4 corners x (int32 depth sum + int32 valid count)
 BYTES_COLOR_EVAL = 32   # 2 boxes x 4 corners x float32
@@ -347,7 +351,7 @@ def serve(forest, seconds):
         gaps = rng.exponential(1.0 / rate, count)
         kinds = rng.choice(len(SERVE_SIZES), count, p=weights / weights.sum())
         which = rng.integers(0, 4, count)
-        srv = cf.Server(forest, hbm_budget_bytes=8 << 30, max_batch_frames=32, max_pending=1 << 16, pipeline_depth=3)
+        srv = cf.Server(forest, hbm_budget_bytes=8 << 30, max_pending=1 << 16, **SERVE_CONFIG)
         # warm the server with one frame of each size
         for w, h, _ in SERVE_SIZES:
             rgb, depth = pool[(w, h)]
@@ -388,7 +392,8 @@ def serve(forest, seconds):
                         "p99_ms_640x480": float(np.percentile(lat[big], 99)) if big.any() else None,
                         "p99_admission_wait_ms": float(np.percentile(qwait, 99)),
                         "batches": c["batches"] - len(SERVE_SIZES), "rejected": c["rejected"]})
-    return {"sizes": "160x120:320x240:640x480:1280x960 = 1:2:4:1", "trees": forest.num_trees, "rates": results}
+    return {"sizes": "160x120:320x240:640x480:1280x960 = 1:2:4:1", "trees": forest.num_trees,
+            "server": dict(SERVE_CONFIG), "rates": results}
 
 
 # ----------------------------------------------------------------------------------------- our arm
@@ -411,7 +416,11 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="Poisson load per offered rate (0: skip)")
     ap.add_argument("--tuning", default="", help="split-search launch shape overrides, e.g. ctas_per_sm=4,"
                     "bins_budget_words=10240 (cf_eval_tuning field names)")
+    ap.add_argument("--serve-config", default="", help="serving overrides, e.g. max_batch_frames=4,pipeline_depth=2")
     args = ap.parse_args()
+    for kv in filter(None, args.serve_config.split(",")):
+        k, v = kv.split("=")
+        SERVE_CONFIG[k.strip()] = int(v)
     W.update(images=args.images, trees=args.trees, max_depth=args.max_depth,
              predict_images=min(args.predict_images, args.images), predict_trees=args.predict_trees)
     if args.impl == "reference":
@@ -535,6 +544,11 @@ def main():
     def forest_e2e(sampler, steps):
         c = train_config()
         c.sampler = sampler
+        # one untimed step first: the first cf_forest_train call of a sampler pays one-time costs
+        # (its device buffers, the sampler's stream and pinned staging)
+        for t in cf.train_forest(ctx, rgb, depth, labels, W["classes"], c, W["trees"]):
+            t.close()
+        barrier()
         t0 = time.perf_counter()
         e2e_evals = 0
         d2h = 0
