@@ -6,7 +6,9 @@
 //   2. for every (sample, feature) pair compute the double response exactly as the reference does,
 //      locate it among the feature's sorted thresholds (binary search on the response rounded up
 //      to float, which orders identically to the reference's double compare) and increment ONE
-//      shared-memory bin [feature][class][position], warp-aggregated with __match_any_sync;
+//      shared-memory bin [feature][class][position] (a plain shared atomic, or warp-aggregated with
+//      __match_any_sync); the lanes of a warp take (sample, feature) pairs of neighbouring samples
+//      (sample groups) or one sample each through the tile's features;
 //   3. turn the bins into cumulative counts, so left(t) = bins up to rank(t), right = node - left;
 //   4. score every (feature, threshold) with the normalised information gain in double and keep
 //      the near-best candidates; a final per-node reduction applies the tie rule.
