@@ -449,6 +449,39 @@ def train_tree(ds, samples, num_classes, config, tree_id=0, seed_counter=0, mode
     return Tree(h), sc.value
 
 
+_ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p)
+
+
+def train_tree_sharded(ds, samples, num_classes, config, rank, world, allgather, tree_id=0, seed_counter=0):
+    """One tree trained by `world` processes together (cf_train_tree_sharded). `allgather(payload: bytes)`
+    must return the concatenation of every rank's payload in rank order (see
+    curfil_b200.distributed.allgather_bytes). Returns (Tree, advanced seed counter)."""
+    samples = np.ascontiguousarray(samples, SAMPLE_DTYPE)
+    errors = []
+
+    def trampoline(send, nbytes, recv, user):
+        try:
+            out = allgather(ctypes.string_at(send, nbytes))
+            if len(out) != nbytes * world:
+                raise ValueError("all-gather returned %d bytes, expected %d" % (len(out), nbytes * world))
+            ctypes.memmove(recv, out, len(out))
+            return 0
+        except Exception as e:  # reported through the status below
+            errors.append(e)
+            return 1
+
+    fn = _ALLGATHER_FN(trampoline)
+    sc = _i32(seed_counter)
+    h = _vp()
+    status = lib().cf_train_tree_sharded(ds.handle, len(samples), _p(samples), int(num_classes), ctypes.byref(config),
+                                         int(tree_id), ctypes.byref(sc), int(rank), int(world), fn, None,
+                                         ctypes.byref(h))
+    if status != 0 and errors:
+        raise errors[0]
+    _check(status)
+    return Tree(h), sc.value
+
+
 def autotune_split_search(ds, samples, num_classes, config, tree_id=0, seed_counter=0, repeats=1, cache=None):
     """Choose the split search's launch shape for this workload (cf_autotune_split_search) and set it on
     the dataset's context. With `cache` (a JSON file path) a previous choice for the same device and

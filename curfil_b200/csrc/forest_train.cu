@@ -15,12 +15,13 @@
 
 #include "host_rng.h"
 #include "sampling.h"
+#include "split_eval.h"
 #include "tree.h"
 
 namespace cf {
 
 cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
-                    int32_t* seed_counter, int mode);
+                    int32_t* seed_counter, int mode, const LevelEvaluator::Shard* shard = nullptr);
 
 namespace {
 

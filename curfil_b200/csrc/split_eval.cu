@@ -761,6 +761,15 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     const int slots = ctx->num_sms * tuning.ctas_per_sm;
     plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_);
     const int n_items = static_cast<int>(h_items_.size());
+    // this process's items: every position of the work order, or positions rank, rank + world, ...
+    const bool sharded = shard.world > 1;
+    h_local_order_.clear();
+    for (int q = sharded ? shard.rank : 0; q < n_items; q += sharded ? shard.world : 1)
+        h_local_order_.push_back(h_order_[q]);
+    const int n_local = static_cast<int>(h_local_order_.size());
+    last_local_evals = 0;
+    for (int id : h_local_order_)
+        last_local_evals += static_cast<int64_t>(node_counts[h_items_[id].node]) * (h_items_[id].f_end - h_items_[id].f_begin);
     items_.reserve(n_items);
     order_.reserve(n_items);
     item_range_.reserve(M + 1);
@@ -768,8 +777,8 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     queue_.reserve(1);
     CF_CUDA_CHECK(cudaMemcpyAsync(items_.get(), h_items_.data(), sizeof(EvalItem) * n_items, cudaMemcpyHostToDevice,
                                   ctx->stream));
-    CF_CUDA_CHECK(cudaMemcpyAsync(order_.get(), h_order_.data(), sizeof(int) * n_items, cudaMemcpyHostToDevice,
-                                  ctx->stream));
+    CF_CUDA_CHECK(cudaMemcpyAsync(order_.get(), h_local_order_.data(), sizeof(int) * std::max(1, n_local),
+                                  cudaMemcpyHostToDevice, ctx->stream));
     CF_CUDA_CHECK(cudaMemcpyAsync(item_range_.get(), h_range_.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice,
                                   ctx->stream));
     CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int), ctx->stream));
@@ -790,15 +799,40 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     args.ranks = lf.ranks.get();
     args.items = items_.get();
     args.order = order_.get();
-    args.n_items = n_items;
+    args.n_items = n_local;
     args.queue = queue_.get();
     args.cands = cands_.get();
     args.ft_max = tuning.ft_max;
     args.bins_budget = budget;
     args.dump_left = dump_left;
-    launch_level_eval(ctx, args, std::min(n_items, slots), tuning);
+    if (n_local > 0) launch_level_eval(ctx, args, std::min(n_local, slots), tuning);
+    if (sharded) exchange(ctx, n_items);
     launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F,
            item_range_.get(), cands_.get(), lf.thr.get(), splits_dev);
+}
+
+// The candidate lists of this process's items go out in work-order position sequence (slot k holds
+// position rank + k x world); the lists of every process come back and are placed by item, so the
+// candidate array equals the one a single process computes.
+void LevelEvaluator::exchange(cf_context* ctx, int n_items) {
+    CF_REQUIRE(shard.allgather != nullptr, "sharded split search: no all-gather function");
+    const int world = shard.world;
+    const int per = (n_items + world - 1) / world;
+    h_cands_.resize(n_items);
+    CF_CUDA_CHECK(cudaMemcpyAsync(h_cands_.data(), cands_.get(), sizeof(ItemCandidates) * n_items,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    h_send_.assign(std::max(1, per), ItemCandidates{});
+    for (int k = 0, q = shard.rank; q < n_items; k++, q += world) h_send_[k] = h_cands_[h_order_[q]];
+    h_recv_.assign(static_cast<size_t>(std::max(1, per)) * world, ItemCandidates{});
+    const size_t bytes = sizeof(ItemCandidates) * std::max(1, per);
+    const int rc = shard.allgather(h_send_.data(), bytes, h_recv_.data(), shard.user);
+    CF_REQUIRE(rc == 0, "sharded split search: the all-gather of candidate lists failed (" + std::to_string(rc) + ")");
+    for (int r = 0; r < world; r++)
+        for (int k = 0, q = r; q < n_items; k++, q += world) h_cands_[h_order_[q]] = h_recv_[static_cast<size_t>(r) * per + k];
+    CF_CUDA_CHECK(cudaMemcpyAsync(cands_.get(), h_cands_.data(), sizeof(ItemCandidates) * n_items,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
 }
 
 void plain_responses(cf_context* ctx, const DsView& ds, const Sample* samples_dev, long long start, int count,

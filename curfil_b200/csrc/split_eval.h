@@ -63,8 +63,22 @@ public:
                   const LevelFeatures& lf, cf_split* splits_dev, uint32_t* dump_left = nullptr);
     EvalTuning tuning;            // the context's tuning at the last evaluate call
     int64_t last_items = 0;
+    int64_t last_local_evals = 0; // feature evaluations this process ran at the last evaluate call
+
+    // Sharding of a level's work items over `world` processes (each holding the same dataset,
+    // samples and candidate table): this process evaluates the items at positions rank, rank+world,
+    // ... of the work order, then one all-gather of the item candidate lists gives every process the
+    // complete list, so the splits equal those of one process.
+    struct Shard {
+        int rank = 0, world = 1;
+        cf_allgather_fn allgather = nullptr;
+        void* user = nullptr;
+    } shard;
 
 private:
+    void exchange(cf_context* ctx, int n_items);
+    std::vector<ItemCandidates> h_cands_, h_send_, h_recv_;
+    std::vector<int> h_local_order_;
     DevArray<EvalItem> items_;
     DevArray<int> order_;
     DevArray<int> item_range_;   // [M + 1] first item of each node

@@ -150,7 +150,7 @@ public:
                                splits_.get());
             }
             CF_CUDA_CHECK(cudaEventRecord(le1, st));
-            evals += n * F;
+            evals += eval_.shard.world > 1 ? eval_.last_local_evals : n * F;
             levels++;
             const bool scatter = level + 1 < cfg_.max_depth;
             const int nxt = 1 - cur;
@@ -230,7 +230,7 @@ private:
 };
 
 cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
-                    int32_t* seed_counter, int mode) {
+                    int32_t* seed_counter, int mode, const LevelEvaluator::Shard* shard) {
     // the dataset keeps one trainer so its device buffers are allocated once, not per tree
     if (ds->trainer == nullptr) {
         ds->trainer = new TreeTrainer(ds, C, cfg, mode);
@@ -238,6 +238,11 @@ cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, cons
     }
     TreeTrainer* trainer = static_cast<TreeTrainer*>(ds->trainer);
     trainer->configure(C, cfg, mode);
+    struct Reset {
+        TreeTrainer* t;
+        ~Reset() { t->eval_.shard = LevelEvaluator::Shard(); }
+    } reset{trainer};
+    trainer->eval_.shard = shard ? *shard : LevelEvaluator::Shard();
     return trainer->train(samples, N, tree_id, seed_counter);
 }
 
@@ -487,7 +492,25 @@ cf_status cf_train_tree(cf_dataset* ds, int num_samples, const cf_sample* sample
         CF_REQUIRE(ds && samples && seed_counter && out, "cf_train_tree: NULL argument");
         validate_config(config);
         CF_REQUIRE(mode == CF_TRAIN_LEVEL_BATCHED || mode == CF_TRAIN_PER_NODE, "cf_train_tree: unknown mode");
-        *out = train_tree(ds, samples, num_samples, num_classes, *config, tree_id, seed_counter, mode);
+        *out = train_tree(ds, samples, num_samples, num_classes, *config, tree_id, seed_counter, mode, nullptr);
+    });
+}
+
+cf_status cf_train_tree_sharded(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                                const cf_train_config* config, int tree_id, int32_t* seed_counter, int rank,
+                                int world, cf_allgather_fn allgather, void* user, cf_tree** out) {
+    return guard([&] {
+        CF_REQUIRE(ds && samples && seed_counter && out, "cf_train_tree_sharded: NULL argument");
+        validate_config(config);
+        CF_REQUIRE(world >= 1 && rank >= 0 && rank < world, "cf_train_tree_sharded: rank must be in [0, world)");
+        CF_REQUIRE(world == 1 || allgather != nullptr, "cf_train_tree_sharded: no all-gather function");
+        LevelEvaluator::Shard shard;
+        shard.rank = rank;
+        shard.world = world;
+        shard.allgather = allgather;
+        shard.user = user;
+        *out = train_tree(ds, samples, num_samples, num_classes, *config, tree_id, seed_counter,
+                          CF_TRAIN_LEVEL_BATCHED, &shard);
     });
 }
 

@@ -6,6 +6,10 @@ source (seed SEED + treeId, random_forest_image.cpp:150-173). So ranks train dis
 collective on the data path, and a forest trained on N ranks is the forest trained on one. The only
 exchange is assembling the forest afterwards: every rank serialises its trees (a few hundred KB each)
 and `gather_forest` all-gathers them, ordered by tree id.
+
+When one tree must span several GPUs, `train_tree_sharded` (with `allgather_bytes`) splits each
+level's work items over the ranks and exchanges their candidate lists once per level; the tree is the
+one a single process trains.
 """
 import io
 
@@ -50,3 +54,21 @@ def gather_forest(local_trees, group=None):
     if len(set(ids)) != len(ids):
         raise RuntimeError("gather_forest: two ranks trained the same tree id")
     return sorted(trees, key=lambda t: t.tree_id)
+
+
+def allgather_bytes(group=None):
+    """An all-gather of equal-size byte strings over torch.distributed, for train_tree_sharded: returns
+    a function payload -> the concatenation of every rank's payload in rank order. NCCL exchanges
+    through the current CUDA device, gloo through host memory."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    device = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else \
+        torch.device("cpu")
+
+    def fn(payload):
+        t = torch.frombuffer(bytearray(payload), dtype=torch.uint8).to(device)
+        out = [torch.empty_like(t) for _ in range(world)]
+        dist.all_gather(out, t, group=group)
+        return b"".join(o.cpu().numpy().tobytes() for o in out)
+    return fn

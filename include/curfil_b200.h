@@ -255,6 +255,21 @@ cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const float* color, c
 cf_status cf_train_tree(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
                         const cf_train_config* config, int tree_id, int32_t* seed_counter, int mode,
                         cf_tree** out);
+/* All-gather of `bytes` bytes from every process of a sharded training: recv receives world x bytes,
+ * process r's contribution at offset r x bytes. Host buffers. Returns 0 on success. */
+typedef int (*cf_allgather_fn)(const void* send, size_t bytes, void* recv, void* user);
+/* One tree trained by `world` processes together (the reference trains a tree on one device; its
+ * multi-device mode assigns whole trees, random_tree_image_gpu.cu:1727). Every process passes the
+ * same dataset contents, samples, configuration, tree id and seed counter. Per level each process
+ * evaluates its share of the level-batched work items (node x feature range; positions rank,
+ * rank + world, ... of the largest-first order), and one call of `allgather` per level exchanges the
+ * items' candidate lists. All processes then hold the same splits, route identically and return the
+ * same tree, identical to cf_train_tree's (level-batched). The exchange is 88 bytes per work item
+ * (about 2.5 MB per level at 200 frames x 2000 features). The tree's feature evaluation count is this
+ * process's share. */
+cf_status cf_train_tree_sharded(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                                const cf_train_config* config, int tree_id, int32_t* seed_counter, int rank,
+                                int world, cf_allgather_fn allgather, void* user, cf_tree** out);
 /* RandomForestImage::train (random_forest_image.cpp:132-182) on raw host frames: GPU integral images,
  * class-uniform sampling (random_tree_image.cpp:911-1059, one host thread), block sort, then
  * cf_train_tree per tree. labels uint8 [n][H][W]; ignored[C] marks ignoredColors. */

@@ -88,3 +88,34 @@ def test_two_gloo_ranks_assemble_the_single_process_forest(tmp_path):
         assert [t.tree_id for t in got] == list(range(num_trees))
         for a, b in zip(got, single):
             _same(a, b)
+
+
+def _allgather_worker(rank, world, port, out_dir):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        fn = D.allgather_bytes()
+        # two rounds, as two levels of a sharded training exchange their candidate lists
+        outs = [fn(bytes([rank + 1 + 10 * k]) * (88 * 3)) for k in range(2)]
+        with open(os.path.join(out_dir, "ag%d.bin" % rank), "wb") as f:
+            f.write(b"".join(outs))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_allgather_bytes_over_two_gloo_ranks(tmp_path):
+    """The all-gather train_tree_sharded calls once per level: every rank receives every rank's
+    payload, in rank order."""
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.start_processes(_allgather_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    want = b"".join(bytes([r + 1 + 10 * k]) * (88 * 3) for k in range(2) for r in range(2))
+    for rank in range(2):
+        with open(os.path.join(str(tmp_path), "ag%d.bin" % rank), "rb") as f:
+            assert f.read() == want
