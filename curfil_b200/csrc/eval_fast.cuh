@@ -96,14 +96,27 @@ __device__ __forceinline__ EvalFeat make_eval_feat(const FeatParams& f) {
     return e;
 }
 
-// Thresholds of one feature in shared memory: sorted ascending; with kPad32 (T <= 31) the row has 32
-// entries, positions T..31 holding +inf, and is searched branch-free in five steps.
+// Thresholds of one feature in shared memory: sorted ascending. With kPad = 32 (T <= 31) or 64
+// (32 <= T <= 63) the row has kPad entries, positions T..kPad-1 holding +inf, and is searched
+// branch-free in five or six steps; kPad = 0 keeps the T thresholds and a binary search.
 constexpr int kPadThresholds = 32;
 
+// the padded row width for T thresholds (0: no padding)
+__host__ __device__ constexpr int padded_row(int T) { return T < 32 ? 32 : (T < 64 ? 64 : 0); }
+
 // #{i : sorted[i] < v}
-template <bool kPad32>
+template <int kPad>
 __device__ __forceinline__ int count_below(const float* sorted, int T, float v) {
-    if (kPad32) {
+    if (kPad == 64) {
+        int k = sorted[31] < v ? 32 : 0;
+        k += sorted[k + 15] < v ? 16 : 0;
+        k += sorted[k + 7] < v ? 8 : 0;
+        k += sorted[k + 3] < v ? 4 : 0;
+        k += sorted[k + 1] < v ? 2 : 0;
+        k += sorted[k] < v ? 1 : 0;
+        return k;
+    }
+    if (kPad == 32) {
         int k = sorted[15] < v ? 16 : 0;
         k += sorted[k + 7] < v ? 8 : 0;
         k += sorted[k + 3] < v ? 4 : 0;
@@ -125,10 +138,10 @@ __device__ __forceinline__ int count_below(const float* sorted, int T, float v) 
 }
 
 // bin of an exact double response: #{t : !(r <= t)}; r <= t (float t) iff RU(r) <= t
-template <bool kPad32>
+template <int kPad>
 __device__ __forceinline__ int exact_bin(double r, const float* sorted, int T) {
     if (isnan(r)) return T;
-    return count_below<kPad32>(sorted, T, __double2float_ru(r));
+    return count_below<kPad>(sorted, T, __double2float_ru(r));
 }
 
 // exact depth response ((s1/1000)/n1 - (s2/1000)/n2 in double, random_tree_image.h:313-315)
@@ -140,17 +153,17 @@ static __device__ __noinline__ double exact_depth_response(int s1, int nv1, int 
 
 // Binning policies of feature_bin.
 // SortedBins: the number of a feature's sorted thresholds t with !(r <= t) (0..T; NaN -> T).
-template <bool kPad32>
+template <int kPad>
 struct SortedBins {
     const float* sorted;
     int T;
     __device__ __forceinline__ int nan() const { return T; }
     // bin of every r in [r0 - delta, r0 + delta] if it is the same for all of them
     __device__ __forceinline__ bool fast(float r0, float delta, int& k) const {
-        k = count_below<kPad32>(sorted, T, r0 - delta);
-        return (!kPad32 && k == T) || sorted[k] > r0 + delta;
+        k = count_below<kPad>(sorted, T, r0 - delta);
+        return (kPad == 0 && k == T) || sorted[k] > r0 + delta;
     }
-    __device__ __forceinline__ int exact(double r) const { return exact_bin<kPad32>(r, sorted, T); }
+    __device__ __forceinline__ int exact(double r) const { return exact_bin<kPad>(r, sorted, T); }
 };
 
 // ThresholdSide: 1 when the sample goes right of one split, !(r <= threshold) (NaN goes right).

@@ -112,7 +112,7 @@ __device__ __noinline__ double score_from_cum(const uint32_t* cum, int stride, c
     return normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, hc)));
 }
 
-template <bool kAgg, bool kPad32, int kMinBlocks, bool kGrouped>
+template <bool kAgg, int kPad, int kMinBlocks, bool kGrouped>
 __global__ void __launch_bounds__(256, kMinBlocks)
 level_eval_kernel(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -130,7 +130,7 @@ level_eval_kernel(EvalArgs a) {
     __shared__ int s_cn;
     __shared__ double s_drop;
 
-    const int TP = kPad32 ? kPadThresholds : a.T;
+    const int TP = kPad ? kPad : a.T;
     // threshold row stride in shared memory: with sample groups the lanes of a warp search different
     // features' rows at the same position, so the rows are skewed by one bank
     const int TPS = TP + (kGrouped ? 1 : 0);
@@ -204,10 +204,11 @@ level_eval_kernel(EvalArgs a) {
             // ---- stage the tile
             for (int i = tid; i < nf; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[f0 + i]);
             const float* g_thr = a.sorted_thr + static_cast<long long>(f0) * T;
-            if (kPad32) {
-                for (int i = tid; i < nf * kPadThresholds; i += blockDim.x) {
-                    const int t = i & (kPadThresholds - 1);
-                    s_thr[(i >> 5) * TPS + t] = t < T ? g_thr[(i >> 5) * T + t] : INFINITY;
+            if (kPad) {
+                constexpr int kShift = kPad == 64 ? 6 : 5;
+                for (int i = tid; i < nf * kPad; i += blockDim.x) {
+                    const int t = i & (kPad - 1);
+                    s_thr[(i >> kShift) * TPS + t] = t < T ? g_thr[(i >> kShift) * T + t] : INFINITY;
                 }
             } else {
                 for (int i = tid; i < nf * T; i += blockDim.x) s_thr[(i / T) * TPS + i % T] = g_thr[i];
@@ -236,7 +237,7 @@ level_eval_kernel(EvalArgs a) {
                     const bool fa = fl < nf;
                     const int fc = fa ? fl : 0;
                     const EvalFeat ef = s_params[fc];
-                    const SortedBins<kPad32> sorted{s_thr + fc * TPS, T};
+                    const SortedBins<kPad> sorted{s_thr + fc * TPS, T};
                     // kUnroll samples per lane and step: their gathers are independent and overlap
                     for (int s0 = warp * SPW; s0 < N; s0 += kUnroll * step) {   // trip count uniform in a warp
                         EvalPixel px[kUnroll];
@@ -280,7 +281,7 @@ level_eval_kernel(EvalArgs a) {
                             const int f = fb + fl;
                             const bool act = sv && f < nf;
                             const int fc = act ? f : 0;
-                            const SortedBins<kPad32> sorted{s_thr + fc * TPS, T};
+                            const SortedBins<kPad> sorted{s_thr + fc * TPS, T};
                             const int row = (fc * cp + lid) * T1;
                             const int key1 = act ? row + feature_bin(px, W, H, s_params[fc], flip == 1, sorted) : -1;
                             bin_increment<kAgg>(s_bins, key1);
@@ -307,8 +308,8 @@ level_eval_kernel(EvalArgs a) {
                 for (; f + 1 < nf; f += 2) {
                     const EvalFeat& fa = s_params[f];
                     const EvalFeat& fb = s_params[f + 1];
-                    const SortedBins<kPad32> sa{s_thr + f * TPS, T};
-                    const SortedBins<kPad32> sb{s_thr + (f + 1) * TPS, T};
+                    const SortedBins<kPad> sa{s_thr + f * TPS, T};
+                    const SortedBins<kPad> sb{s_thr + (f + 1) * TPS, T};
                     const int row_a = (f * cp + lid) * T1;
                     const int row_b = row_a + cp * T1;
                     const int ka = row_a + feature_bin(px, W, H, fa, flip == 1, sa);
@@ -324,7 +325,7 @@ level_eval_kernel(EvalArgs a) {
                 }
                 if (f < nf) {
                     const EvalFeat& fp = s_params[f];
-                    const SortedBins<kPad32> sorted{s_thr + f * TPS, T};
+                    const SortedBins<kPad> sorted{s_thr + f * TPS, T};
                     const int row = (f * cp + lid) * T1;
                     const int key1 = row + feature_bin(px, W, H, fp, flip == 1, sorted);
                     bin_increment<kAgg>(s_bins, key1);
@@ -351,7 +352,7 @@ level_eval_kernel(EvalArgs a) {
                         const Sample smp = tail[s];
                         const EvalPixel px = make_eval_pixel(a.ds, smp);
                         const EvalFeat& fp = s_params[f];
-                        const SortedBins<kPad32> sorted{s_thr + f * TPS, T};
+                        const SortedBins<kPad> sorted{s_thr + f * TPS, T};
                         const int row = (f * cp + s_lid[smp.label]) * T1;
                         key1 = row + feature_bin(px, W, H, fp, smp.flip == 1, sorted);
                         if (smp.flip == 2) key2 = row + feature_bin(px, W, H, fp, true, sorted);
@@ -642,7 +643,7 @@ __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const 
 // Shared-memory layout of a level_eval launch; budget = histogram words (at least one feature).
 SmemLayout level_eval_smem(int C, int T, const EvalTuning& tuning, int* budget) {
     *budget = std::max(tuning.bins_budget_words, C * (T + 1));
-    const int TP = T < kPadThresholds ? kPadThresholds : T;
+    const int TP = padded_row(T) ? padded_row(T) : T;
     return SmemLayout(C, T, TP + 1, tuning.ft_max, *budget);   // rows skewed by one bank with sample groups
 }
 
@@ -659,40 +660,45 @@ void set_level_eval_smem(K kernel, size_t smem, int ctas) {
     CF_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
 }
 
-template <bool kAgg, bool kPad32, bool kGrouped>
+template <bool kAgg, int kPad, bool kGrouped>
 void launch_level_eval_g(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm) {
     if (ctas_per_sm >= 4) {
-        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 4, kGrouped>, smem, ctas_per_sm);
-        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 4, kGrouped>, args);
+        set_level_eval_smem(level_eval_kernel<kAgg, kPad, 4, kGrouped>, smem, ctas_per_sm);
+        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad, 4, kGrouped>, args);
     } else {
-        set_level_eval_smem(level_eval_kernel<kAgg, kPad32, 3, kGrouped>, smem, ctas_per_sm);
-        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad32, 3, kGrouped>, args);
+        set_level_eval_smem(level_eval_kernel<kAgg, kPad, 3, kGrouped>, smem, ctas_per_sm);
+        launch(ctx, "level_eval", dim3(grid), dim3(256), smem, level_eval_kernel<kAgg, kPad, 3, kGrouped>, args);
     }
 }
 
-template <bool kAgg, bool kPad32>
+template <bool kAgg, int kPad>
 void launch_level_eval_t(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm,
                          bool grouped) {
-    if (grouped) launch_level_eval_g<kAgg, kPad32, true>(ctx, args, grid, smem, ctas_per_sm);
-    else launch_level_eval_g<kAgg, kPad32, false>(ctx, args, grid, smem, ctas_per_sm);
+    if (grouped) launch_level_eval_g<kAgg, kPad, true>(ctx, args, grid, smem, ctas_per_sm);
+    else launch_level_eval_g<kAgg, kPad, false>(ctx, args, grid, smem, ctas_per_sm);
 }
 
-// The level_eval instance for the tuning and threshold count (T <= 31 takes the padded search).
+template <bool kAgg>
+void launch_level_eval_a(cf_context* ctx, const EvalArgs& args, int grid, size_t smem, int ctas_per_sm,
+                         bool grouped) {
+    switch (padded_row(args.T)) {
+        case 32: launch_level_eval_t<kAgg, 32>(ctx, args, grid, smem, ctas_per_sm, grouped); break;
+        case 64: launch_level_eval_t<kAgg, 64>(ctx, args, grid, smem, ctas_per_sm, grouped); break;
+        default: launch_level_eval_t<kAgg, 0>(ctx, args, grid, smem, ctas_per_sm, grouped); break;
+    }
+}
+
+// The level_eval instance for the tuning and threshold count (T <= 31 and 32 <= T <= 63 take the
+// padded branch-free searches).
 void launch_level_eval(cf_context* ctx, const EvalArgs& args, int grid, const EvalTuning& tuning) {
     int budget = 0;
     const SmemLayout lay = level_eval_smem(args.C, args.T, tuning, &budget);
     CF_REQUIRE(lay.total + 4096 <= ctx->smem_per_block_optin,
                "split search: classes x thresholds too large for shared memory");
     CF_REQUIRE(args.bins_budget == budget && args.ft_max == tuning.ft_max, "split search: inconsistent tuning");
-    const bool pad = args.T < kPadThresholds;
     const bool g = tuning.sample_groups != 0;
-    if (tuning.warp_aggregate) {
-        if (pad) launch_level_eval_t<true, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
-        else launch_level_eval_t<true, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
-    } else {
-        if (pad) launch_level_eval_t<false, true>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
-        else launch_level_eval_t<false, false>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
-    }
+    if (tuning.warp_aggregate) launch_level_eval_a<true>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
+    else launch_level_eval_a<false>(ctx, args, grid, lay.total, tuning.ctas_per_sm, g);
 }
 
 }  // namespace
