@@ -57,11 +57,47 @@ __device__ __forceinline__ int fast_norm(int v, float av, float d, float inv_d) 
     return v < 0 ? -r : r;
 }
 
+// Two fast_norm evaluations in packed f32x2 arithmetic (sm_100): the same operations and roundings
+// per value as fast_norm, two values per instruction.
+__device__ __forceinline__ unsigned long long pack_f2(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void unpack_f2(unsigned long long v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ void fast_norm2(int v0, int v1, float av0, float av1, float d, float inv_d, int& r0,
+                                           int& r1) {
+    const unsigned long long a = pack_f2(av0, av1), inv = pack_f2(inv_d, inv_d);
+    const unsigned long long em = pack_f2(-4.76837158203125e-07f, -4.76837158203125e-07f);
+    const unsigned long long ep = pack_f2(4.76837158203125e-07f, 4.76837158203125e-07f);
+    const unsigned long long big = pack_f2(8388608.0f, 8388608.0f);
+    unsigned long long q, lo, hi, tl, th;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(q) : "l"(a), "l"(inv));
+    asm("fma.rm.f32x2 %0, %1, %2, %1;" : "=l"(lo) : "l"(q), "l"(em));   // q (1 - 2^-21), rounded down
+    asm("fma.rp.f32x2 %0, %1, %2, %1;" : "=l"(hi) : "l"(q), "l"(ep));   // q (1 + 2^-21), rounded up
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(tl) : "l"(lo), "l"(big));     // 2^23 + floor(lo)
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(th) : "l"(hi), "l"(big));
+    float tl0, tl1, th0, th1;
+    unpack_f2(tl, tl0, tl1);
+    unpack_f2(th, th0, th1);
+    int a0 = __float_as_int(tl0) - 0x4B000000, a1 = __float_as_int(tl1) - 0x4B000000;
+    if (tl0 != th0) a0 = exact_norm_abs(av0, d);
+    if (tl1 != th1) a1 = exact_norm_abs(av1, d);
+    r0 = v0 < 0 ? -a0 : a0;
+    r1 = v1 < 0 ? -a1 : a1;
+}
+
 // Normalisation policies of feature_bin.
-// CheckedNorm: fast_norm, each value checked on its own.
+// CheckedNorm: fast_norm, each value checked on its own; pair() scales two values at once.
 struct CheckedNorm {
     __device__ __forceinline__ int operator()(int v, float av, float d, float inv_d) const {
         return fast_norm(v, av, d, inv_d);
+    }
+    __device__ __forceinline__ void pair(int v0, int v1, float av0, float av1, float d, float inv_d, int& r0,
+                                         int& r1) const {
+        fast_norm2(v0, v1, av0, av1, d, inv_d, r0, r1);
     }
 };
 
@@ -184,15 +220,15 @@ __device__ __forceinline__ int feature_bin(const EvalPixel& p, int W, int H, con
     if (!(p.d > 0.0f)) return T;
     const int o1x = flip ? -f.v[0] : f.v[0];
     const int o2x = flip ? -f.v[2] : f.v[2];
-    const int x1 = p.x + norm(o1x, f.av[0], p.d, p.inv_d);
-    const int y1 = p.y + norm(f.v[1], f.av[1], p.d, p.inv_d);
-    const int w1 = max(1, norm(f.v[4], f.av[4], p.d, p.inv_d));
-    const int h1 = max(1, norm(f.v[5], f.av[5], p.d, p.inv_d));
+    int nx1, ny1, nw1, nh1;
+    norm.pair(o1x, f.v[1], f.av[0], f.av[1], p.d, p.inv_d, nx1, ny1);
+    norm.pair(f.v[4], f.v[5], f.av[4], f.av[5], p.d, p.inv_d, nw1, nh1);
+    const int x1 = p.x + nx1, y1 = p.y + ny1, w1 = max(1, nw1), h1 = max(1, nh1);
     if (x1 - w1 < 0 || x1 + w1 >= W || y1 - h1 < 0 || y1 + h1 >= H) return T;
-    const int x2 = p.x + norm(o2x, f.av[2], p.d, p.inv_d);
-    const int y2 = p.y + norm(f.v[3], f.av[3], p.d, p.inv_d);
-    const int w2 = max(1, norm(f.v[6], f.av[6], p.d, p.inv_d));
-    const int h2 = max(1, norm(f.v[7], f.av[7], p.d, p.inv_d));
+    int nx2, ny2, nw2, nh2;
+    norm.pair(o2x, f.v[3], f.av[2], f.av[3], p.d, p.inv_d, nx2, ny2);
+    norm.pair(f.v[6], f.v[7], f.av[6], f.av[7], p.d, p.inv_d, nw2, nh2);
+    const int x2 = p.x + nx2, y2 = p.y + ny2, w2 = max(1, nw2), h2 = max(1, nh2);
     if (x2 - w2 < 0 || x2 + w2 >= W || y2 - h2 < 0 || y2 + h2 >= H) return T;
     const int ul1 = (y1 - h1) * W + (x1 - w1), ur1 = (y1 - h1) * W + (x1 + w1);
     const int ll1 = (y1 + h1) * W + (x1 - w1), lr1 = (y1 + h1) * W + (x1 + w1);
