@@ -112,17 +112,27 @@ struct cf_server {
                         break;
                     }
                 if (!slot) continue;
-                // admission: frames in arrival order while they fit in the slot's budget
+                // admission: frames in the policy's order (arrival, or smallest first with requests
+                // older than max_wait_ms ahead) while they fit in the slot's budget
                 size_t dev = 0, host = 0;
+                const double now = now_ms();
                 while (!queue.empty() && static_cast<int>(batch.size()) < cfg.max_batch_frames) {
-                    auto& r = queue.front();
+                    size_t pick = 0;
+                    if (cfg.policy == 1 && now - queue.front()->submit_ms <= cfg.max_wait_ms) {
+                        // the queue is in arrival order: the front is the oldest, so no request is overdue
+                        for (size_t i = 1; i < queue.size(); i++)
+                            if (static_cast<long long>(queue[i]->W) * queue[i]->H <
+                                static_cast<long long>(queue[pick]->W) * queue[pick]->H)
+                                pick = i;
+                    }
+                    auto r = queue[pick];
                     const size_t d = frame_device_bytes(r->W, r->H, forest->C, cfg.return_probabilities != 0);
                     const size_t h = frame_host_bytes(r->W, r->H, forest->C, cfg.return_probabilities != 0);
                     if (dev + d > slot_bytes || host + h > slot_host_bytes) break;
                     dev += d;
                     host += h;
                     batch.push_back(r);
-                    queue.pop_front();
+                    queue.erase(queue.begin() + static_cast<long>(pick));
                 }
                 if (batch.empty()) continue;
                 slot->busy = true;
@@ -284,6 +294,8 @@ cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf
         CF_REQUIRE(config->hbm_budget_bytes > 0 && config->max_batch_frames >= 1 && config->max_pending >= 1 &&
                        config->pipeline_depth >= 1,
                    "cf_server_create: invalid configuration");
+        CF_REQUIRE(config->policy == 0 || (config->policy == 1 && config->max_wait_ms > 0.0f),
+                   "cf_server_create: policy is 0 (arrival order) or 1 (smallest first, max_wait_ms > 0)");
         cf_context* ctx = forest->ctx;
         make_current(ctx);
         std::unique_ptr<cf_server> s(new cf_server());

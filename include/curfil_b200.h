@@ -388,6 +388,9 @@ typedef struct cf_server_config {
     int32_t max_pending;        /* queue length before submits are rejected */
     int32_t pipeline_depth;     /* batches in flight on the device */
     int32_t return_probabilities;
+    int32_t policy;             /* admission order: 0 arrival; 1 smallest frame first, except that a request
+                                   waiting longer than max_wait_ms goes first (no frame waits for ever) */
+    float max_wait_ms;          /* age limit of policy 1 */
 } cf_server_config;
 
 typedef struct cf_request_stats {

@@ -83,3 +83,44 @@ def test_admission_rejects_oversized_and_unknown(forest):
         server.wait(123456789, (1, 1), timeout_s=0.01)
     assert server.counters()["rejected"] == 1
     server.close()
+
+
+def _burst(forest, policy, max_wait_ms):
+    server = cf.Server(forest, hbm_budget_bytes=2 << 30, max_batch_frames=1, pipeline_depth=1, policy=policy,
+                       max_wait_ms=max_wait_ms)
+    frames = {}
+    for k, (w, h) in enumerate(SIZES):
+        rgb, depth, _ = cf.synthetic_frames(700 + k, 1, w, h, 12, 10)
+        frames[(w, h)] = (rgb[0], depth[0])
+    order = [SIZES[3], SIZES[2], SIZES[1], SIZES[0]] * 4
+    ids = [(key, server.submit(*frames[key])) for key in order]
+    got = []
+    for key, rid in ids:
+        labels, _, st = server.wait(rid, frames[key][1].shape)
+        _, alone = forest.predict(*frames[key], probabilities=False)
+        np.testing.assert_array_equal(labels, alone[0])
+        got.append((st.batch_id, key[0] * key[1], rid))
+    server.close()
+    return sorted(got)
+
+
+def _mean_rank(got, px):
+    return np.mean([i for i, (_, p, _) in enumerate(got) if p == px])
+
+
+def test_smallest_first_policy_orders_queued_frames_by_size(forest):
+    # submitted largest first in every group of four: in arrival order the 1280x960 frames run earlier
+    # on average than the 160x120 ones; smallest first reverses that (requests that arrive while
+    # earlier ones run make the exact order depend on timing, the averages do not)
+    fifo = _burst(forest, 0, 0.0)
+    assert _mean_rank(fifo, 1280 * 960) < _mean_rank(fifo, 160 * 120)
+    assert [rid for _, _, rid in fifo] == sorted(rid for _, _, rid in fifo)
+    sjf = _burst(forest, 1, 1e6)
+    assert _mean_rank(sjf, 160 * 120) < _mean_rank(sjf, 1280 * 960)
+    # every request overdue at once: arrival order again
+    aged = _burst(forest, 1, 1e-3)
+    assert [rid for _, _, rid in aged] == sorted(rid for _, _, rid in aged)
+    with pytest.raises(cf.CurfilError):
+        cf.Server(forest, policy=1, max_wait_ms=0.0)
+    with pytest.raises(cf.CurfilError):
+        cf.Server(forest, policy=2, max_wait_ms=1.0)
