@@ -618,7 +618,10 @@ def main():
                 "predict": predict,
                 "per_node": per_node,
                 "levels_tree0": [[n, s, round(ms, 3)] for n, s, ms in trees[0].level_stats()],
-                "feature_evals_per_step": total_evals / args.steps}
+                "feature_evals_per_step": total_evals / args.steps,
+                # split evaluations: every feature evaluation is binned against all T thresholds
+                "split_evals_per_s": value * W["thresholds"],
+                "per_node_split_evals_per_s": per_node["value"] * W["thresholds"] if per_node else None}
         print(json.dumps(line), flush=True)
     ds.close()
     ctx.close()
