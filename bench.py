@@ -36,11 +36,12 @@ W = dict(images=200, width=640, height=480, cells=40, classes=40, samples_per_im
          predict_trees=10, seed=2026)
 # serving: Poisson arrivals of mixed frame sizes (weights 1:2:4:1) at these offered rates
 SERVE_RATES = (200, 1000, 4000)
-# cf_server_config of the serving runs: one 640x480 frame already fills the GPU, so small batches cost
-# no throughput and keep a frame from waiting for a long batch (p99 at 1000 frames/s: 12 ms with 2
-# frames per batch, 20 ms with 32); smallest frames first (with a 20 ms age limit) lets 640x480 frames
-# pass queued 1280x960 ones (p99 of 640x480 frames at 1000 frames/s: 8.7 ms against 10.8 ms)
-SERVE_CONFIG = dict(max_batch_frames=2, pipeline_depth=3, policy=1, max_wait_ms=20.0)
+# cf_server_config of the serving runs: one 640x480 frame already fills the GPU, so one frame per batch
+# costs no throughput and keeps a frame from waiting for a long batch; smallest frames first (with a
+# 20 ms age limit) lets small frames pass queued large ones, and device priorities let their thread
+# blocks pass a large frame already running. At 1000 frames/s this moves the p99 of 640x480 frames from
+# 8.8 to 6.0 ms and of 160x120 frames from 6.4 to 1.6 ms; 1280x960 frames wait longer (17 -> 18 ms).
+SERVE_CONFIG = dict(max_batch_frames=1, pipeline_depth=6, policy=1, max_wait_ms=20.0, device_priority=1)
 SERVE_SIZES = ((160, 120, 1), (320, 240, 2), (640, 480, 4), (1280, 960, 1))
 BYTES_DEPTH_EVAL = 64   # 2 boxes x 4 corners x (int32 depth sum + int32 valid count)
 BYTES_COLOR_EVAL = 32   # 2 boxes x 4 corners x float32
@@ -383,6 +384,9 @@ def serve(forest, seconds):
         lat = np.array([done[r][2] - done[r][0] for r in ids])
         qwait = np.array([done[r][1] - done[r][0] for r in ids])
         big = np.array([done[r][3] == (480, 640) for r in ids])
+        shapes = np.array([done[r][3] for r in ids])
+        by_size = {f"{w}x{h}": float(np.percentile(lat[(shapes[:, 0] == h) & (shapes[:, 1] == w)], 99))
+                   for w, h, _ in SERVE_SIZES if ((shapes[:, 0] == h) & (shapes[:, 1] == w)).any()}
         span = (max(done[r][2] for r in ids) - min(done[r][0] for r in ids)) / 1e3
         pxs = sum(done[r][3][0] * done[r][3][1] for r in ids)
         c = srv.counters()
@@ -391,6 +395,7 @@ def serve(forest, seconds):
                         "mpx_per_s": pxs / span / 1e6, "p50_ms": float(np.percentile(lat, 50)),
                         "p99_ms": float(np.percentile(lat, 99)),
                         "p99_ms_640x480": float(np.percentile(lat[big], 99)) if big.any() else None,
+                        "p99_ms_by_size": by_size,
                         "p99_admission_wait_ms": float(np.percentile(qwait, 99)),
                         "batches": c["batches"] - len(SERVE_SIZES), "rejected": c["rejected"]})
     return {"sizes": "160x120:320x240:640x480:1280x960 = 1:2:4:1", "trees": forest.num_trees,

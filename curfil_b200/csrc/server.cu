@@ -5,9 +5,13 @@
 // queued. A launcher thread forms batches from whatever is queued when a pipeline slot frees up:
 // frames of any size are admitted while the slot's share of the device-memory budget holds them,
 // copied host->device through pinned staging, integrated, and classified by ONE launch over all
-// frames of the batch; results come back device->host on the same slot stream. A completion thread
-// waits for each slot's event in order and publishes the results. With several slots, one batch's
-// copies overlap another batch's kernels, and requests arriving during a launch join the next batch.
+// frames of the batch; results come back device->host on the same slot stream. Each slot has a waiter
+// thread that publishes the slot's results as soon as its event completes, in whatever order the slots
+// finish. With several slots, one batch's copies overlap another batch's kernels, and requests arriving
+// during a launch join the next batch. With device priorities on, each batch goes to the server's
+// stream for its size class (one stream per CUDA priority level, chosen by the batch's pixel count), so
+// the thread blocks of a small batch are dispatched ahead of a large batch's blocks that have not
+// started yet, and batches of one class run in arrival order.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -50,17 +54,40 @@ size_t frame_host_bytes(int W, int H, int C, bool probs) {
     return up(px * 3) + up(px * 2) + up(px) + (probs ? up(px * 4 * C) : 0);
 }
 
+// Pixel count of the most urgent device-priority level (one 160x120 frame); each further level holds
+// batches up to four times larger.
+constexpr long long kUrgentPixels = 160 * 120;
+
+// Device-priority level of a batch of `px` pixels among `levels` (0 most urgent).
+int priority_level(long long px, int levels) {
+    int b = 0;
+    while (px > kUrgentPixels && b + 1 < levels) {
+        px = (px + 3) / 4;
+        b++;
+    }
+    return b;
+}
+
 struct Slot {
-    cudaStream_t stream = nullptr;
+    // the streams this slot's batches may run on (not owned): its own stream, or with device priorities
+    // the server's streams of each level, most urgent first, shared by all slots. A slot's buffers are
+    // reused only after its previous batch's event has completed on the host, so no stream has to keep
+    // one slot's batches in order.
+    std::vector<cudaStream_t> streams;
+    cudaStream_t stream = nullptr;       // the stream of the batch in flight
     cudaEvent_t done = nullptr;
+    cudaEvent_t copied = nullptr;        // the batch's inputs are on the device (with a copy stream)
     DeviceBuffer dev;
     PinnedBuffer host;
+    PinnedBuffer desc;                   // the batch's FrameDesc array, staged for the copy
     DevArray<FrameDesc> frames;
     std::vector<FrameDesc> h_frames;
     std::vector<std::shared_ptr<Request>> batch;
     std::vector<size_t> host_off;   // per frame: offset of rgb in host staging
     int batch_id = -1;
-    bool busy = false;
+    bool busy = false;       // admitted a batch (set by the launcher, cleared when its results are out)
+    bool launched = false;   // the batch's work is enqueued and `done` recorded behind it
+    std::thread waiter;      // publishes this slot's batches as each completes, in any order across slots
 };
 
 }  // namespace
@@ -74,14 +101,19 @@ struct cf_server {
     cf_server_config cfg{};
     size_t slot_bytes = 0, slot_host_bytes = 0;
     std::vector<std::unique_ptr<Slot>> slots;
+    // Every stream the server created. With device priorities there is one stream per level, shared by
+    // the slots: CUDA maps streams onto a few hardware queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 by
+    // default), and a stream for each slot and level would put a small batch in the same queue as, and
+    // behind, a large one.
+    std::vector<cudaStream_t> owned_streams;
+    cudaStream_t copy_stream = nullptr;   // host->device inputs of every batch (with device priorities)
     std::mutex mu;
     std::condition_variable cv_queue, cv_slot, cv_done, cv_inflight;
     std::deque<std::shared_ptr<Request>> queue;
     std::unordered_map<int64_t, std::shared_ptr<Request>> requests;
-    std::deque<Slot*> inflight;
     int64_t next_id = 1, submitted = 0, completed = 0, rejected = 0, batches = 0;
     bool stopping = false;
-    std::thread launcher, completer;
+    std::thread launcher;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     std::string fatal;
 
@@ -146,20 +178,26 @@ struct cf_server {
             try {
                 run_batch(slot, batch, batch_id);
             } catch (const std::exception& e) {
+                // whatever was enqueued must finish before the slot's buffers are handed out again,
+                // possibly to a batch on another of its streams
+                if (copy_stream) cudaStreamSynchronize(copy_stream);
+                if (slot->stream) cudaStreamSynchronize(slot->stream);
                 std::lock_guard<std::mutex> lk(mu);
                 for (auto& r : batch) {
                     r->status = CF_ERR_CUDA;
                     r->error = e.what();
                     r->done = true;
                 }
+                slot->batch.clear();
                 slot->busy = false;
                 cv_done.notify_all();
                 cv_slot.notify_all();
+                cv_inflight.notify_all();
                 continue;
             }
             {
                 std::lock_guard<std::mutex> lk(mu);
-                inflight.push_back(slot);
+                slot->launched = true;
                 batches++;
             }
             cv_inflight.notify_all();
@@ -177,6 +215,19 @@ struct cf_server {
         slot->host_off.resize(batch.size());
         slot->batch = batch;
         slot->batch_id = batch_id;
+        long long batch_px = 0;
+        for (auto& r : batch) batch_px += static_cast<long long>(r->W) * r->H;
+        slot->stream = slot->streams[priority_level(batch_px, static_cast<int>(slot->streams.size()))];
+        // inputs go on the copy stream when there is one, so they do not queue behind the kernels
+        // already waiting in the batch's (shared) priority stream
+        cudaStream_t in = copy_stream ? copy_stream : slot->stream;
+        struct Planes {
+            const uint8_t* rgb;
+            uint16_t* depth;
+            float* color;
+            int2* integral;
+        };
+        std::vector<Planes> planes(batch.size());
         int blocks = 0;
         for (size_t i = 0; i < batch.size(); i++) {
             Request& r = *batch[i];
@@ -204,9 +255,9 @@ struct cf_server {
             std::memcpy(h_depth, r.depth.data(), px * 2);
             hoff += up(px * 2);
             hoff += up(px) + (want_probs ? up(px * 4 * C) : 0);
-            CF_CUDA_CHECK(cudaMemcpyAsync(d_rgb, h_rgb, px * 3, cudaMemcpyHostToDevice, slot->stream));
-            CF_CUDA_CHECK(cudaMemcpyAsync(d_depth, h_depth, px * 2, cudaMemcpyHostToDevice, slot->stream));
-            integrate_frames(ctx, d_rgb, d_depth, 1, r.W, r.H, d_color, d_int, slot->stream, forest->preprocess);
+            CF_CUDA_CHECK(cudaMemcpyAsync(d_rgb, h_rgb, px * 3, cudaMemcpyHostToDevice, in));
+            CF_CUDA_CHECK(cudaMemcpyAsync(d_depth, h_depth, px * 2, cudaMemcpyHostToDevice, in));
+            planes[i] = {d_rgb, d_depth, d_color, d_int};
             FrameDesc& fr = slot->h_frames[i];
             fr.color = d_color;
             fr.depth = d_int;
@@ -218,8 +269,19 @@ struct cf_server {
             fr.pad = 0;
             blocks += classify_blocks_for(r.W, r.H);
         }
-        CF_CUDA_CHECK(cudaMemcpyAsync(slot->frames.get(), slot->h_frames.data(), sizeof(FrameDesc) * batch.size(),
-                                      cudaMemcpyHostToDevice, slot->stream));
+        // the descriptors go through pinned memory: a copy from pageable memory may wait for the stream
+        std::memcpy(slot->desc.get(), slot->h_frames.data(), sizeof(FrameDesc) * batch.size());
+        CF_CUDA_CHECK(cudaMemcpyAsync(slot->frames.get(), slot->desc.get(), sizeof(FrameDesc) * batch.size(),
+                                      cudaMemcpyHostToDevice, in));
+        if (in != slot->stream) {
+            CF_CUDA_CHECK(cudaEventRecord(slot->copied, in));
+            CF_CUDA_CHECK(cudaStreamWaitEvent(slot->stream, slot->copied, 0));
+        }
+        for (size_t i = 0; i < batch.size(); i++) {
+            const Planes& pl = planes[i];
+            integrate_frames(ctx, pl.rgb, pl.depth, 1, batch[i]->W, batch[i]->H, pl.color, pl.integral, slot->stream,
+                             forest->preprocess);
+        }
         classify_frames(ctx, forest, slot->frames.get(), static_cast<int>(batch.size()), blocks, slot->stream);
         for (size_t i = 0; i < batch.size(); i++) {
             Request& r = *batch[i];
@@ -233,18 +295,16 @@ struct cf_server {
         CF_CUDA_CHECK(cudaEventRecord(slot->done, slot->stream));
     }
 
-    void complete_loop() {
+    // One waiter per slot: a batch's results are published when its own event completes, so a small
+    // batch that finishes first is not held behind a larger one launched before it.
+    void complete_loop(Slot* slot) {
         cudaSetDevice(ctx->device);
         for (;;) {
-            Slot* slot = nullptr;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_inflight.wait(lk, [&] { return stopping || !inflight.empty(); });
-                if (inflight.empty()) {
-                    if (stopping) return;
-                    continue;
-                }
-                slot = inflight.front();
+                // a busy slot that is not yet launched is between admission and enqueue: wait for it
+                cv_inflight.wait(lk, [&] { return slot->launched || (stopping && !slot->busy); });
+                if (!slot->launched) return;
             }
             const cudaError_t e = cudaEventSynchronize(slot->done);
             const double t = now_ms();
@@ -278,7 +338,7 @@ struct cf_server {
                 }
                 slot->batch.clear();
                 slot->busy = false;
-                inflight.pop_front();
+                slot->launched = false;
             }
             cv_done.notify_all();
             cv_slot.notify_all();
@@ -296,6 +356,8 @@ cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf
                    "cf_server_create: invalid configuration");
         CF_REQUIRE(config->policy == 0 || (config->policy == 1 && config->max_wait_ms > 0.0f),
                    "cf_server_create: policy is 0 (arrival order) or 1 (smallest first, max_wait_ms > 0)");
+        CF_REQUIRE(config->device_priority == 0 || config->device_priority == 1,
+                   "cf_server_create: device_priority is 0 or 1");
         cf_context* ctx = forest->ctx;
         make_current(ctx);
         std::unique_ptr<cf_server> s(new cf_server());
@@ -305,18 +367,45 @@ cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf
         s->slot_bytes = static_cast<size_t>(config->hbm_budget_bytes) / config->pipeline_depth;
         // host staging mirrors the device share (inputs and outputs only)
         s->slot_host_bytes = s->slot_bytes;
+        // device-priority levels: greatest (most urgent) .. least, or the default priority alone
+        int least = 0, greatest = 0;
+        if (config->device_priority) CF_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        std::vector<cudaStream_t> level_streams;
+        for (int l = 0; config->device_priority && l <= least - greatest; l++) {
+            cudaStream_t st = nullptr;
+            CF_CUDA_CHECK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, greatest + l));
+            s->owned_streams.push_back(st);
+            level_streams.push_back(st);
+        }
+        if (config->device_priority) {
+            CF_CUDA_CHECK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+            s->owned_streams.push_back(s->copy_stream);
+        }
         for (int i = 0; i < config->pipeline_depth; i++) {
             auto slot = std::make_unique<Slot>();
-            CF_CUDA_CHECK(cudaStreamCreateWithFlags(&slot->stream, cudaStreamNonBlocking));
+            if (config->device_priority) {
+                slot->streams = level_streams;
+            } else {
+                cudaStream_t st = nullptr;
+                CF_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                s->owned_streams.push_back(st);
+                slot->streams.push_back(st);
+            }
+            slot->stream = slot->streams[0];
             CF_CUDA_CHECK(cudaEventCreateWithFlags(&slot->done, cudaEventDisableTiming));
+            CF_CUDA_CHECK(cudaEventCreateWithFlags(&slot->copied, cudaEventDisableTiming));
             slot->dev.reserve(s->slot_bytes);
             slot->host.reserve(s->slot_host_bytes);
+            slot->desc.reserve(sizeof(FrameDesc) * config->max_batch_frames);
             slot->frames.reserve(config->max_batch_frames);
             s->slots.push_back(std::move(slot));
         }
         cf_server* raw = s.get();
+        for (auto& slot : s->slots) {
+            Slot* sl = slot.get();
+            sl->waiter = std::thread([raw, sl] { raw->complete_loop(sl); });
+        }
         s->launcher = std::thread([raw] { raw->launch_loop(); });
-        s->completer = std::thread([raw] { raw->complete_loop(); });
         context_retain(ctx);
         *out = s.release();
     });
@@ -342,17 +431,23 @@ cf_status cf_server_destroy(cf_server* server) {
         // drain batches still on the device
         {
             std::unique_lock<std::mutex> lk(server->mu);
-            server->cv_done.wait_for(lk, std::chrono::seconds(60), [&] { return server->inflight.empty(); });
+            server->cv_done.wait_for(lk, std::chrono::seconds(60), [&] {
+                for (auto& s : server->slots)
+                    if (s->busy) return false;
+                return true;
+            });
         }
         server->cv_inflight.notify_all();
-        if (server->completer.joinable()) server->completer.join();
+        for (auto& s : server->slots)
+            if (s->waiter.joinable()) s->waiter.join();
         cudaSetDevice(server->ctx->device);
+        for (cudaStream_t st : server->owned_streams) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
         for (auto& s : server->slots) {
-            if (s->stream) {
-                cudaStreamSynchronize(s->stream);
-                cudaStreamDestroy(s->stream);
-            }
             if (s->done) cudaEventDestroy(s->done);
+            if (s->copied) cudaEventDestroy(s->copied);
         }
         cf_context* ctx = server->ctx;
         delete server;

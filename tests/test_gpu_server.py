@@ -124,3 +124,27 @@ def test_smallest_first_policy_orders_queued_frames_by_size(forest):
         cf.Server(forest, policy=1, max_wait_ms=0.0)
     with pytest.raises(cf.CurfilError):
         cf.Server(forest, policy=2, max_wait_ms=1.0)
+
+
+def test_device_priority_streams_same_results(forest):
+    # four slots, batches of one or two frames on streams of different CUDA priority, results published
+    # per slot as each completes: every request still gets exactly its frame's direct prediction
+    server = cf.Server(forest, hbm_budget_bytes=2 << 30, max_batch_frames=2, pipeline_depth=4,
+                       return_probabilities=True, policy=1, max_wait_ms=50.0, device_priority=1)
+    frames = {}
+    for k, (w, h) in enumerate(SIZES):
+        rgb, depth, _ = cf.synthetic_frames(900 + k, 1, w, h, 12, 10)
+        frames[(w, h)] = (rgb[0], depth[0])
+    direct = {key: forest.predict(*f) for key, f in frames.items()}
+    order = [SIZES[3], SIZES[0], SIZES[2], SIZES[1], SIZES[0], SIZES[2], SIZES[3], SIZES[1]] * 3
+    ids = [(key, server.submit(*frames[key])) for key in order]
+    for key, rid in ids:
+        labels, probs, st = server.wait(rid, frames[key][1].shape, probabilities=True)
+        np.testing.assert_array_equal(labels, direct[key][1][0])
+        np.testing.assert_array_equal(probs, direct[key][0][0])
+        assert st.submit_ms <= st.admitted_ms <= st.done_ms
+    c = server.counters()
+    assert c["completed"] == c["submitted"] == len(order)
+    server.close()
+    with pytest.raises(cf.CurfilError):
+        cf.Server(forest, device_priority=2)
