@@ -60,6 +60,8 @@ struct EvalArgs {
     ItemCandidates* cands;
     int ft_max;
     int bins_budget;
+    uint32_t* group_bins;  // [groups][bins_budget] merged counts of chunked items, zero at launch
+    int* group_count;      // [groups] chunks finished, zero at launch
     uint32_t* dump_left;   // optional [M][F][T][C] left counts (tests); nullptr in training
 };
 
@@ -129,6 +131,7 @@ level_eval_kernel(EvalArgs a) {
     __shared__ int s_ct[kMaxCand], s_cf[kMaxCand];
     __shared__ int s_cn;
     __shared__ double s_drop;
+    __shared__ int s_last;
 
     const int TP = kPad ? kPad : a.T;
     // threshold row stride in shared memory: with sample groups the lanes of a warp search different
@@ -195,7 +198,10 @@ level_eval_kernel(EvalArgs a) {
         const int cp = s_cp;
         const double total = s_total;
         const double hc = s_hc;
-        const int N = nd.count;
+        // the item's samples: the whole node, or one chunk of it
+        const bool chunked = item.chunks > 1;
+        const int N = chunked ? item.s_end - item.s_begin : nd.count;
+        const long long sbase = nd.start + (chunked ? item.s_begin : 0);
         int ft = a.bins_budget / (cp * T1);
         ft = max(1, min(ft, a.ft_max));
 
@@ -247,7 +253,7 @@ level_eval_kernel(EvalArgs a) {
                         for (int u = 0; u < kUnroll; u++) {
                             const int s = s0 + js + u * step;
                             act[u] = fa && s < N;
-                            const Sample m = a.samples[nd.start + min(s, N - 1)];
+                            const Sample m = a.samples[sbase + min(s, N - 1)];
                             px[u] = make_eval_pixel(a.ds, m);
                             row[u] = (fc * cp + s_lid[m.label]) * T1;
                             flip[u] = act[u] ? m.flip : 0;
@@ -272,7 +278,7 @@ level_eval_kernel(EvalArgs a) {
                     for (int s0 = warp * SPW; s0 < N; s0 += step) {
                         const int s = s0 + js;
                         const bool sv = s < N;
-                        const Sample smp = a.samples[nd.start + min(s, N - 1)];
+                        const Sample smp = a.samples[sbase + min(s, N - 1)];
                         const EvalPixel px = make_eval_pixel(a.ds, smp);
                         const int lid = s_lid[smp.label];
                         const int flip = smp.flip;
@@ -297,7 +303,7 @@ level_eval_kernel(EvalArgs a) {
             // ---- histogram, sample-major over whole blocks of samples: each thread keeps one sample
             // and walks the tile's features, so the sample's neighbourhood is reused from L1
             for (int s0 = 0; s0 < n_major; s0 += nthr) {
-                const Sample smp = a.samples[nd.start + s0 + tid];
+                const Sample smp = a.samples[sbase + s0 + tid];
                 const EvalPixel px = make_eval_pixel(a.ds, smp);
                 const int lid = s_lid[smp.label];
                 const int flip = smp.flip;
@@ -339,7 +345,7 @@ level_eval_kernel(EvalArgs a) {
             // all threads with a uniform trip count so warps stay converged
             const int Nt = N - n_major;
             if (!kGrouped && Nt > 0) {
-                const Sample* tail = a.samples + nd.start + n_major;
+                const Sample* tail = a.samples + sbase + n_major;
                 const long long pairs = static_cast<long long>(nf) * Nt;
                 const int iters = static_cast<int>((pairs + nthr - 1) / nthr);
                 const int qstep = nthr / Nt;
@@ -368,6 +374,26 @@ level_eval_kernel(EvalArgs a) {
                 }
             }
             __syncthreads();
+
+            if (chunked) {
+                // ---- one chunk of the node's samples (the item is a single tile): add its counts to
+                // the group's histogram in global memory and count the chunk in; the chunk that
+                // arrives last loads the merged counts and scores them, the others leave the item with
+                // no candidates. Integer sums, so the merged counts do not depend on the order.
+                uint32_t* g = a.group_bins + static_cast<long long>(item.group) * a.bins_budget;
+                for (int i = tid; i < nbins; i += blockDim.x) {
+                    const uint32_t v = s_bins[i];
+                    if (v) atomicAdd(g + i, v);
+                }
+                __threadfence();
+                __syncthreads();
+                if (tid == 0) s_last = atomicAdd(a.group_count + item.group, 1) == item.chunks - 1 ? 1 : 0;
+                __syncthreads();
+                if (!s_last) break;
+                __threadfence();
+                for (int i = tid; i < nbins; i += blockDim.x) s_bins[i] = __ldcg(g + i);
+                __syncthreads();
+            }
 
             // ---- cumulative counts along the threshold positions
             for (int row = tid; row < nf * cp; row += blockDim.x) {
@@ -721,33 +747,60 @@ EvalTuning EvalTuning::of(cf_context* ctx) {
 }
 
 void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
-                      std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order) {
+                      std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
+                      int chunk_features, int* n_groups) {
     const int M = static_cast<int>(node_counts.size());
     const int g = std::max(1, tuning.feature_granule);
     long long total_work = 0;
     for (int n : node_counts) total_work += static_cast<long long>(n) * F;
     const double target_items = tuning.items_per_slot * slots;
     const double work_per_item = std::max(1.0, static_cast<double>(total_work) / target_items);
+    // features per item of each node
+    std::vector<int> per(M);
+    long long plain_items = 0;
+    for (int n = 0; n < M; n++) {
+        const double w = static_cast<double>(node_counts[n]) * F;
+        int parts = static_cast<int>(std::ceil(w / work_per_item));
+        parts = std::max(1, std::min(parts, (F + g - 1) / g));
+        per[n] = ((((F + parts - 1) / parts) + g - 1) / g) * g;
+        plain_items += (F + per[n] - 1) / per[n];
+    }
+    // sample chunks where the level has too few items to fill the resident CTAs
+    const long long want = static_cast<long long>(kChunkItemsPerSlot) * slots;
+    const int k = chunk_features > 0 && plain_items < want ? static_cast<int>((want + plain_items - 1) / plain_items) : 1;
+    int groups = 0;
     items.clear();
     range.assign(M + 1, 0);
     std::vector<long long> work;
     for (int n = 0; n < M; n++) {
         range[n] = static_cast<int>(items.size());
-        const double w = static_cast<double>(node_counts[n]) * F;
-        int parts = static_cast<int>(std::ceil(w / work_per_item));
-        parts = std::max(1, std::min(parts, (F + g - 1) / g));
-        int per = (F + parts - 1) / parts;
-        per = ((per + g - 1) / g) * g;
-        for (int f0 = 0; f0 < F; f0 += per) {
+        const int chunks = std::min(k, node_counts[n] / kMinChunkSamples);
+        const int pf = chunks > 1 ? std::min(per[n], chunk_features) : per[n];
+        for (int f0 = 0; f0 < F; f0 += pf) {
             EvalItem it;
             it.node = n;
             it.f_begin = f0;
-            it.f_end = std::min(F, f0 + per);
+            it.f_end = std::min(F, f0 + pf);
+            it.chunks = std::max(1, chunks);
+            it.s_begin = 0;
+            it.s_end = node_counts[n];
+            it.group = -1;
             it.pad = 0;
-            items.push_back(it);
-            work.push_back(static_cast<long long>(node_counts[n]) * (it.f_end - it.f_begin));
+            if (chunks <= 1) {
+                items.push_back(it);
+                work.push_back(static_cast<long long>(node_counts[n]) * (it.f_end - it.f_begin));
+                continue;
+            }
+            it.group = groups++;
+            for (int c = 0; c < chunks; c++) {
+                it.s_begin = static_cast<int>(static_cast<long long>(node_counts[n]) * c / chunks);
+                it.s_end = static_cast<int>(static_cast<long long>(node_counts[n]) * (c + 1) / chunks);
+                items.push_back(it);
+                work.push_back(static_cast<long long>(it.s_end - it.s_begin) * (it.f_end - it.f_begin));
+            }
         }
     }
+    if (n_groups) *n_groups = groups;
     range[M] = static_cast<int>(items.size());
     const int n_items = static_cast<int>(items.size());
     order.resize(n_items);
@@ -765,17 +818,24 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     if (M == 0) return;
     tuning = EvalTuning::of(ctx);
     const int slots = ctx->num_sms * tuning.ctas_per_sm;
-    plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_);
+    const bool sharded = shard.world > 1;
+    int budget = 0;
+    level_eval_smem(C, T, tuning, &budget);
+    // sample chunks of a node's items merge their counts on this device, so they are not sharded; a
+    // chunked item covers at most the features of the smallest tile (all C classes present)
+    const int chunk_features = sharded ? 0 : std::max(1, std::min(tuning.ft_max, budget / (C * (T + 1))));
+    int n_groups = 0;
+    plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups);
     const int n_items = static_cast<int>(h_items_.size());
     // this process's items: every position of the work order, or positions rank, rank + world, ...
-    const bool sharded = shard.world > 1;
     h_local_order_.clear();
     for (int q = sharded ? shard.rank : 0; q < n_items; q += sharded ? shard.world : 1)
         h_local_order_.push_back(h_order_[q]);
     const int n_local = static_cast<int>(h_local_order_.size());
     last_local_evals = 0;
     for (int id : h_local_order_)
-        last_local_evals += static_cast<int64_t>(node_counts[h_items_[id].node]) * (h_items_[id].f_end - h_items_[id].f_begin);
+        last_local_evals += static_cast<int64_t>(h_items_[id].s_end - h_items_[id].s_begin) *
+                            (h_items_[id].f_end - h_items_[id].f_begin);
     items_.reserve(n_items);
     order_.reserve(n_items);
     item_range_.reserve(M + 1);
@@ -788,10 +848,15 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     CF_CUDA_CHECK(cudaMemcpyAsync(item_range_.get(), h_range_.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice,
                                   ctx->stream));
     CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int), ctx->stream));
+    if (n_groups > 0) {
+        group_bins_.reserve(static_cast<size_t>(n_groups) * budget);
+        group_count_.reserve(n_groups);
+        CF_CUDA_CHECK(cudaMemsetAsync(group_bins_.get(), 0, sizeof(uint32_t) * n_groups * static_cast<size_t>(budget),
+                                      ctx->stream));
+        CF_CUDA_CHECK(cudaMemsetAsync(group_count_.get(), 0, sizeof(int) * n_groups, ctx->stream));
+    }
     last_items = n_items;
 
-    int budget = 0;
-    level_eval_smem(C, T, tuning, &budget);
     EvalArgs args;
     args.ds = ds;
     args.samples = samples;
@@ -810,6 +875,8 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     args.cands = cands_.get();
     args.ft_max = tuning.ft_max;
     args.bins_budget = budget;
+    args.group_bins = n_groups > 0 ? group_bins_.get() : nullptr;
+    args.group_count = n_groups > 0 ? group_count_.get() : nullptr;
     args.dump_left = dump_left;
     if (n_local > 0) launch_level_eval(ctx, args, std::min(n_local, slots), tuning);
     if (sharded) exchange(ctx, n_items);
@@ -1099,6 +1166,8 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         args.cands = d_cands;
         args.ft_max = tuning.ft_max;
         args.bins_budget = budget;
+        args.group_bins = nullptr;   // planned without sample chunks
+        args.group_count = nullptr;
         args.dump_left = nullptr;
         launch_level_eval(ctx, args, std::min(n_items, slots), tuning);
         launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F, d_range,

@@ -17,6 +17,13 @@ struct EvalItem {
     int node;
     int f_begin;
     int f_end;
+    // chunks > 1: the item covers samples [s_begin, s_end) of the node and is one of `chunks` items of
+    // group `group` (same node and features); each adds its counts to the group's histogram in global
+    // memory, and the one that finishes last scores the merged counts
+    int chunks;
+    int s_begin;
+    int s_end;
+    int group;
     int pad;
 };
 
@@ -51,8 +58,15 @@ struct EvalTuning {
 
 // Work items of one level: node n is cut into feature ranges so that the level yields about
 // items_per_slot items per resident CTA; order lists the items by decreasing work (samples x features).
+// With chunk_features > 0 and fewer than kChunkItemsPerSlot items per resident CTA (the top levels,
+// where one or a few nodes hold every sample), the items of nodes with at least 2 x kMinChunkSamples
+// samples cover at most chunk_features features (one histogram tile) and are cut into sample chunks;
+// *n_groups receives the number of chunk groups.
+constexpr int kChunkItemsPerSlot = 4;
+constexpr int kMinChunkSamples = 4096;
 void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
-                      std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order);
+                      std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
+                      int chunk_features = 0, int* n_groups = nullptr);
 
 class LevelEvaluator {
 public:
@@ -84,6 +98,8 @@ private:
     DevArray<int> item_range_;   // [M + 1] first item of each node
     DevArray<ItemCandidates> cands_;
     DevArray<int> queue_;
+    DevArray<uint32_t> group_bins_;   // [groups][bins budget] merged counts of chunked items
+    DevArray<int> group_count_;       // [groups] chunks finished
     std::vector<EvalItem> h_items_;
     std::vector<int> h_order_;
     std::vector<int> h_range_;
