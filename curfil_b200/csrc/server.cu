@@ -8,10 +8,10 @@
 // frames of the batch; results come back device->host on the same slot stream. Each slot has a waiter
 // thread that publishes the slot's results as soon as its event completes, in whatever order the slots
 // finish. With several slots, one batch's copies overlap another batch's kernels, and requests arriving
-// during a launch join the next batch. With device priorities on, each batch goes to the server's
-// stream for its size class (one stream per CUDA priority level, chosen by the batch's pixel count), so
-// the thread blocks of a small batch are dispatched ahead of a large batch's blocks that have not
-// started yet, and batches of one class run in arrival order.
+// during a launch join the next batch. With device priorities on, a batch holds frames of one size
+// class and goes to the server's stream for that class (one stream per CUDA priority level, chosen by
+// the frame's pixel count), so the thread blocks of small frames are dispatched ahead of a large
+// frame's blocks that have not started yet, and batches of one class run in admission order.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -55,10 +55,10 @@ size_t frame_host_bytes(int W, int H, int C, bool probs) {
 }
 
 // Pixel count of the most urgent device-priority level (one 160x120 frame); each further level holds
-// batches up to four times larger.
+// frames up to four times larger.
 constexpr long long kUrgentPixels = 160 * 120;
 
-// Device-priority level of a batch of `px` pixels among `levels` (0 most urgent).
+// Device-priority level (size class) of a frame of `px` pixels among `levels` (0 most urgent).
 int priority_level(long long px, int levels) {
     int b = 0;
     while (px > kUrgentPixels && b + 1 < levels) {
@@ -106,6 +106,7 @@ struct cf_server {
     // default), and a stream for each slot and level would put a small batch in the same queue as, and
     // behind, a large one.
     std::vector<cudaStream_t> owned_streams;
+    int levels = 1;                       // device-priority levels (1 without device priorities)
     cudaStream_t copy_stream = nullptr;   // host->device inputs of every batch (with device priorities)
     std::mutex mu;
     std::condition_variable cv_queue, cv_slot, cv_done, cv_inflight;
@@ -148,6 +149,7 @@ struct cf_server {
                 // older than max_wait_ms ahead) while they fit in the slot's budget
                 size_t dev = 0, host = 0;
                 const double now = now_ms();
+                int level = -1;   // with device priorities a batch holds frames of one size class
                 while (!queue.empty() && static_cast<int>(batch.size()) < cfg.max_batch_frames) {
                     size_t pick = 0;
                     if (cfg.policy == 1 && now - queue.front()->submit_ms <= cfg.max_wait_ms) {
@@ -158,6 +160,11 @@ struct cf_server {
                                 pick = i;
                     }
                     auto r = queue[pick];
+                    if (cfg.device_priority) {
+                        const int l = priority_level(static_cast<long long>(r->W) * r->H, levels);
+                        if (level >= 0 && l != level) break;
+                        level = l;
+                    }
                     const size_t d = frame_device_bytes(r->W, r->H, forest->C, cfg.return_probabilities != 0);
                     const size_t h = frame_host_bytes(r->W, r->H, forest->C, cfg.return_probabilities != 0);
                     if (dev + d > slot_bytes || host + h > slot_host_bytes) break;
@@ -215,9 +222,10 @@ struct cf_server {
         slot->host_off.resize(batch.size());
         slot->batch = batch;
         slot->batch_id = batch_id;
-        long long batch_px = 0;
-        for (auto& r : batch) batch_px += static_cast<long long>(r->W) * r->H;
-        slot->stream = slot->streams[priority_level(batch_px, static_cast<int>(slot->streams.size()))];
+        // the size class of the batch's largest frame (with device priorities all its frames share one)
+        long long frame_px = 0;
+        for (auto& r : batch) frame_px = std::max(frame_px, static_cast<long long>(r->W) * r->H);
+        slot->stream = slot->streams[priority_level(frame_px, static_cast<int>(slot->streams.size()))];
         // inputs go on the copy stream when there is one, so they do not queue behind the kernels
         // already waiting in the batch's (shared) priority stream
         cudaStream_t in = copy_stream ? copy_stream : slot->stream;
@@ -378,6 +386,7 @@ cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf
             level_streams.push_back(st);
         }
         if (config->device_priority) {
+            s->levels = static_cast<int>(level_streams.size());
             CF_CUDA_CHECK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
             s->owned_streams.push_back(s->copy_stream);
         }

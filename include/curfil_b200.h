@@ -391,10 +391,10 @@ typedef struct cf_server_config {
     int32_t policy;             /* admission order: 0 arrival; 1 smallest frame first, except that a request
                                    waiting longer than max_wait_ms goes first (no frame waits for ever) */
     float max_wait_ms;          /* age limit of policy 1 */
-    int32_t device_priority;    /* 1: each batch runs on a stream whose CUDA priority rises as its pixel count
-                                   falls (one level per factor 4), so the thread blocks of a small batch are
-                                   scheduled ahead of those still waiting in a larger batch's launch; 0: one
-                                   priority for all */
+    int32_t device_priority;    /* 1: a batch holds frames of one size class (one class per factor 4 in pixels)
+                                   and runs on a stream whose CUDA priority rises as the class's frames get
+                                   smaller, so the thread blocks of small frames are scheduled ahead of those
+                                   still waiting in a larger frame's launch; 0: one priority for all */
 } cf_server_config;
 
 typedef struct cf_request_stats {
