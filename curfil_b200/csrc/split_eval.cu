@@ -748,7 +748,7 @@ EvalTuning EvalTuning::of(cf_context* ctx) {
 
 void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
                       std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
-                      int chunk_features, int* n_groups) {
+                      int chunk_features, int* n_groups, int max_groups) {
     const int M = static_cast<int>(node_counts.size());
     const int g = std::max(1, tuning.feature_granule);
     long long total_work = 0;
@@ -774,7 +774,11 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
     std::vector<long long> work;
     for (int n = 0; n < M; n++) {
         range[n] = static_cast<int>(items.size());
-        const int chunks = std::min(k, node_counts[n] / kMinChunkSamples);
+        int chunks = std::min(k, node_counts[n] / kMinChunkSamples);
+        if (chunks > 1) {
+            const int node_groups = (F + std::min(per[n], chunk_features) - 1) / std::min(per[n], chunk_features);
+            if (groups + node_groups > max_groups) chunks = 1;   // over the group memory limit: whole-node items
+        }
         const int pf = chunks > 1 ? std::min(per[n], chunk_features) : per[n];
         for (int f0 = 0; f0 < F; f0 += pf) {
             EvalItem it;
@@ -825,7 +829,9 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     // chunked item covers at most the features of the smallest tile (all C classes present)
     const int chunk_features = sharded ? 0 : std::max(1, std::min(tuning.ft_max, budget / (C * (T + 1))));
     int n_groups = 0;
-    plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups);
+    const int max_groups = static_cast<int>(kMaxChunkGroupBytes / (sizeof(uint32_t) * static_cast<size_t>(budget)));
+    plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups,
+                     max_groups);
     const int n_items = static_cast<int>(h_items_.size());
     // this process's items: every position of the work order, or positions rank, rank + world, ...
     h_local_order_.clear();

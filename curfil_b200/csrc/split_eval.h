@@ -60,13 +60,15 @@ struct EvalTuning {
 // items_per_slot items per resident CTA; order lists the items by decreasing work (samples x features).
 // With chunk_features > 0 and fewer than kChunkItemsPerSlot items per resident CTA (the top levels,
 // where one or a few nodes hold every sample), the items of nodes with at least 2 x kMinChunkSamples
-// samples cover at most chunk_features features (one histogram tile) and are cut into sample chunks;
-// *n_groups receives the number of chunk groups.
+// samples cover at most chunk_features features (one histogram tile) and are cut into sample chunks,
+// for at most max_groups groups (nodes past the limit keep whole-node items); *n_groups receives the
+// number of chunk groups.
 constexpr int kChunkItemsPerSlot = 4;
 constexpr int kMinChunkSamples = 4096;
+constexpr size_t kMaxChunkGroupBytes = size_t(64) << 20;   // merged histograms of one level's chunk groups
 void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
                       std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
-                      int chunk_features = 0, int* n_groups = nullptr);
+                      int chunk_features = 0, int* n_groups = nullptr, int max_groups = 0);
 
 class LevelEvaluator {
 public:
