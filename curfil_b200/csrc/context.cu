@@ -20,6 +20,7 @@ void destroy_context_now(cf_context* ctx) {
             cudaEventDestroy(pr.second);
         }
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    if (ctx->spare_trainer && ctx->spare_trainer_free) ctx->spare_trainer_free(ctx->spare_trainer);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }

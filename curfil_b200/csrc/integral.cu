@@ -207,6 +207,15 @@ cf_status cf_dataset_destroy(cf_dataset* ds) {
         cf_context* ctx = ds->ctx;
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        {
+            // the dataset's training buffers stay with the context for the next dataset
+            std::lock_guard<std::mutex> lock(ctx->mu);
+            if (ds->trainer && ctx->spare_trainer == nullptr) {
+                ctx->spare_trainer = ds->trainer;
+                ctx->spare_trainer_free = ds->trainer_free;
+                ds->trainer = nullptr;
+            }
+        }
         delete ds;
         cf::context_release(ctx);
     });

@@ -48,6 +48,7 @@ void validate_thresholds(const float* thr, long long n) {
 class TreeTrainer {
 public:
     TreeTrainer(cf_dataset* ds, int C, const cf_train_config& cfg, int mode) : ds_(ds), C_(C), cfg_(cfg), mode_(mode) {}
+    void rebind(cf_dataset* ds) { ds_ = ds; }   // the buffers are the dataset-independent state
     void configure(int C, const cf_train_config& cfg, int mode) {
         C_ = C;
         cfg_ = cfg;
@@ -232,6 +233,18 @@ private:
 cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
                     int32_t* seed_counter, int mode, const LevelEvaluator::Shard* shard) {
     // the dataset keeps one trainer so its device buffers are allocated once, not per tree
+    if (ds->trainer == nullptr) {
+        // the buffers of a destroyed dataset's trainer, if the context keeps some
+        cf_context* ctx = ds->ctx;
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        if (ctx->spare_trainer) {
+            ds->trainer = ctx->spare_trainer;
+            ds->trainer_free = ctx->spare_trainer_free;
+            ctx->spare_trainer = nullptr;
+            ctx->spare_trainer_free = nullptr;
+            static_cast<TreeTrainer*>(ds->trainer)->rebind(ds);
+        }
+    }
     if (ds->trainer == nullptr) {
         ds->trainer = new TreeTrainer(ds, C, cfg, mode);
         ds->trainer_free = [](void* p) { delete static_cast<TreeTrainer*>(p); };
