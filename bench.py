@@ -410,7 +410,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="timed cf_forest_train calls (after one untimed call) for the end-to-end figure")
     ap.add_argument("--no-per-node", action="store_true", help="skip the plain per-node comparison tree")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default split-search launch shape")
     # workload size (defaults: the full-size configuration); smaller cases are for profiler captures
