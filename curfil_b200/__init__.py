@@ -450,6 +450,62 @@ def train_tree(ds, samples, num_classes, config, tree_id=0, seed_counter=0, mode
     return Tree(h), sc.value
 
 
+class LevelSnapshot:
+    """cf_level_snapshot: the input state of one level of a tree's training, which can be trained
+    again on its own (candidate generation, split search, routing)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        lv, m, n = _i32(), _i32(), _i64()
+        _check(lib().cf_level_snapshot_info(handle, ctypes.byref(lv), ctypes.byref(m), ctypes.byref(n)))
+        self.level, self.num_nodes, self.num_samples = lv.value, m.value, n.value
+
+    def export(self):
+        """(node_offsets int64 [M+1], samples [n], level seed)."""
+        offsets = np.empty(self.num_nodes + 1, np.int64)
+        samples = np.empty(self.num_samples, SAMPLE_DTYPE)
+        seed = ctypes.c_uint32()
+        _check(lib().cf_level_snapshot_export(self.handle, _p(offsets), _p(samples), ctypes.byref(seed)))
+        return offsets, samples, seed.value
+
+    def run(self, mode=LEVEL_BATCHED, splits=False):
+        """Trains the level again; returns dict(ms, evals, next_nodes, next_samples[, splits])."""
+        ms, ev, nn, ns = ctypes.c_double(), _i64(), _i32(), _i64()
+        best = np.empty(self.num_nodes, SPLIT_DTYPE) if splits else None
+        _check(lib().cf_level_snapshot_run(self.handle, int(mode), _p(best), ctypes.byref(ms), ctypes.byref(ev),
+                                           ctypes.byref(nn), ctypes.byref(ns)))
+        out = dict(ms=ms.value, evals=ev.value, next_nodes=nn.value, next_samples=ns.value)
+        if splits:
+            out["splits"] = best
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().cf_level_snapshot_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def train_tree_snapshots(ds, samples, num_classes, config, levels, tree_id=0, seed_counter=0):
+    """cf_train_tree_snapshots: (Tree, [LevelSnapshot of each listed level the tree reaches],
+    advanced seed counter)."""
+    samples = np.ascontiguousarray(samples, SAMPLE_DTYPE)
+    lv = np.ascontiguousarray(levels, np.int32)
+    handles = (_vp * max(1, len(lv)))()
+    got = _i32()
+    sc = _i32(seed_counter)
+    h = _vp()
+    _check(lib().cf_train_tree_snapshots(ds.handle, len(samples), _p(samples), int(num_classes),
+                                         ctypes.byref(config), int(tree_id), ctypes.byref(sc), len(lv), _p(lv),
+                                         handles, ctypes.byref(got), ctypes.byref(h)))
+    return Tree(h), [LevelSnapshot(_vp(handles[i])) for i in range(got.value)], sc.value
+
+
 _ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p)
 
 

@@ -1031,11 +1031,45 @@ constexpr int kNoAllocMaxFeatures = 16384;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// Status bits of the input check (noalloc_check_kernel).
+constexpr int kBadImage = 1, kBadPixel = 2, kBadLabel = 4, kBadFlip = 8, kBadThreshold = 16;
+
+// Checks the caller's device inputs before the split search reads them: every sample's image index,
+// pixel, flip setting and label (the label must be counted in its node's histogram, because the
+// kernel keeps histogram rows only for the classes a node's histogram holds), and every threshold
+// (NaN would corrupt the sorted thresholds). Sets bits of *status; reads only checked indexes.
+__global__ void noalloc_check_kernel(const Sample* __restrict__ samples, long long n,
+                                     const NodeDesc* __restrict__ nodes, int M, const uint32_t* __restrict__ hist,
+                                     int C, int num_images, int W, int H, const float* __restrict__ thr,
+                                     long long n_thr, int* status) {
+    int bad = 0;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+        const Sample s = samples[i];
+        if (s.image >= static_cast<uint32_t>(num_images)) bad |= kBadImage;
+        if (s.x >= W || s.y >= H) bad |= kBadPixel;
+        if (s.flip > 2) bad |= kBadFlip;
+        // the node owning sample i: the last node whose start is <= i (starts ascend, node 0 at 0)
+        int lo = 0, hi = M - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (nodes[mid].start <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        if (s.label >= C || hist[static_cast<long long>(lo) * C + s.label] == 0u) bad |= kBadLabel;
+    }
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n_thr; i += stride)
+        if (isnan(thr[i])) bad |= kBadThreshold;
+    if (bad) atomicOr(status, bad);
+}
+
 struct NoAllocLayout {
-    size_t nodes, items, order, range, cands, queue, packs, sorted, ranks, total;
+    size_t status, nodes, items, order, range, cands, queue, packs, sorted, ranks, total;
     NoAllocLayout(int M, int n_items, int F, int T) {
         auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
         size_t o = 0;
+        status = o;
+        o += a(sizeof(int));
         nodes = o;
         o += a(sizeof(NodeDesc) * M);
         items = o;
@@ -1058,20 +1092,15 @@ struct NoAllocLayout {
     }
 };
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[128] = {};
-
-// Device address of the scratch array on `device` (the current device). Host code cannot use the
-// array's name as a device address, so it is looked up once per device and cached.
-char* noalloc_scratch(int device) {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    CF_REQUIRE(device >= 0 && device < 128, "allocation-free split search: device index out of range");
-    if (g_noalloc_addr[device] == nullptr) {
-        void* p = nullptr;
-        CF_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_addr[device] = p;
-    }
-    return static_cast<char*>(g_noalloc_addr[device]);
+// Device address of the scratch array on the current device. In host code the array's name is a
+// host-side stand-in, not a device address, so the address is looked up with the device current.
+// The lookup is made on every call (it is cheap once the module is loaded), so no cached address
+// outlives a device reset; the first call on a device loads the module, which is why that call
+// should come before any stream capture.
+char* noalloc_scratch() {
+    void* p = nullptr;
+    CF_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    return static_cast<char*>(p);
 }
 
 }  // namespace
@@ -1096,6 +1125,7 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
                        static_cast<long long>(num_features) * num_thresholds <= kNoAllocMaxFeatureThresholds,
                    "cf_evaluate_best_splits_noalloc: features x thresholds beyond the fixed scratch "
                    "(at most 16384 features and 2^20 feature-threshold pairs)");
+        CF_REQUIRE(num_thresholds <= 4096, "cf_evaluate_best_splits_noalloc: thresholds must be in [1, 4096]");
         CF_REQUIRE(node_offsets[0] == 0, "cf_evaluate_best_splits_noalloc: node offsets must start at 0");
         make_current(ctx);
         const int M = num_nodes, F = num_features, T = num_thresholds, C = num_classes;
@@ -1125,7 +1155,8 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         const NoAllocLayout lay(M, n_items, F, T);
         CF_REQUIRE(lay.total <= kNoAllocScratchBytes, "cf_evaluate_best_splits_noalloc: level too large for the "
                                                       "16 MiB fixed scratch");
-        char* base = noalloc_scratch(ctx->device);
+        char* base = noalloc_scratch();
+        int* d_status = reinterpret_cast<int*>(base + lay.status);
         NodeDesc* d_nodes = reinterpret_cast<NodeDesc*>(base + lay.nodes);
         EvalItem* d_items = reinterpret_cast<EvalItem*>(base + lay.items);
         int* d_order = reinterpret_cast<int*>(base + lay.order);
@@ -1140,8 +1171,30 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         CF_CUDA_CHECK(cudaMemcpyAsync(d_items, items.data(), sizeof(EvalItem) * n_items, cudaMemcpyHostToDevice, st));
         CF_CUDA_CHECK(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * n_items, cudaMemcpyHostToDevice, st));
         CF_CUDA_CHECK(cudaMemcpyAsync(d_range, range.data(), sizeof(int) * (M + 1), cudaMemcpyHostToDevice, st));
-        // the work queue counter is the only scratch word that must start at zero
+        // the work queue counter and the check's status word are the scratch words that must start at
+        // zero (the array keeps the previous call's contents)
         CF_CUDA_CHECK(cudaMemsetAsync(d_queue, 0, sizeof(int), st));
+        CF_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+        // the caller's inputs are checked on the device before the split search indexes with them
+        {
+            const long long n = node_offsets[M];
+            const long long n_thr = static_cast<long long>(F) * T;
+            const long long work = std::max(n, n_thr);
+            const int blocks = static_cast<int>(std::min<long long>((work + 255) / 256, 4LL * ctx->num_sms));
+            launch(ctx, "noalloc_check", dim3(blocks), dim3(256), 0, noalloc_check_kernel,
+                   reinterpret_cast<const Sample*>(samples), n, static_cast<const NodeDesc*>(d_nodes), M,
+                   node_histograms, C, num_images, width, height, thresholds, n_thr, d_status);
+            int status = 0;
+            CF_CUDA_CHECK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CF_CUDA_CHECK(cudaStreamSynchronize(st));
+            std::string why;
+            if (status & kBadImage) why += " image index >= num_images;";
+            if (status & kBadPixel) why += " pixel outside the image;";
+            if (status & kBadLabel) why += " label >= num_classes or not counted in its node's histogram;";
+            if (status & kBadFlip) why += " flip setting > 2;";
+            if (status & kBadThreshold) why += " NaN threshold;";
+            CF_REQUIRE(status == 0, "cf_evaluate_best_splits_noalloc: invalid input:" + why);
+        }
         launch(ctx, "prepare_features", dim3((F + 7) / 8), dim3(256), 0, prepare_eval_features_kernel, F, T, features,
                thresholds, d_packs, d_sorted, d_ranks);
 

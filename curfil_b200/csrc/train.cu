@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
 
 #include "host_rng.h"
@@ -44,6 +45,32 @@ void validate_thresholds(const float* thr, long long n) {
 }
 
 }  // namespace
+
+}  // namespace cf
+
+// The input state of one level of a tree's training (the loop body of RandomTreeTrain::train,
+// random_tree.h:1262-1410): the level's node-contiguous samples, their node indices, the open nodes
+// and their histograms, and the level seed, so the level can be trained again on its own.
+struct cf_level_snapshot {
+    cf_dataset* ds = nullptr;
+    int level = 0, M = 0, C = 0, tree_next = 0;
+    long long n = 0;
+    uint32_t seed = 0;
+    cf_train_config cfg{};
+    std::vector<int> counts;              // samples per open node (host)
+    std::vector<int64_t> offsets;         // [M + 1] node offsets into the level's samples (host)
+    cf::DevArray<cf::Sample> samples;
+    cf::DevArray<int> snode;
+    cf::DevArray<cf::NodeDesc> nodes;
+    cf::DevArray<uint32_t> hist;
+    // results of the last run
+    float last_ms = 0;
+    int64_t last_evals = 0;
+    int next_nodes = 0;
+    long long next_samples = 0;
+};
+
+namespace cf {
 
 class TreeTrainer {
 public:
@@ -134,6 +161,8 @@ public:
             CF_CUDA_CHECK(cudaStreamSynchronize(st));
             counts.resize(M);
             for (int i = 0; i < M; i++) counts[i] = h_nodes[i].count;
+            if (captured_ && std::find(capture_.begin(), capture_.end(), level) != capture_.end())
+                captured_->push_back(snapshot(cur, level, M, n, seed, tree_next, counts, h_nodes));
             cudaEvent_t le0, le1;
             CF_CUDA_CHECK(cudaEventCreate(&le0));
             CF_CUDA_CHECK(cudaEventCreate(&le1));
@@ -210,9 +239,103 @@ public:
         return t;
     }
 
+    // Levels (root = 1) whose input state the next train() call copies into snapshots.
+    void capture(const std::vector<int>& levels, std::vector<cf_level_snapshot*>* out) {
+        capture_ = levels;
+        captured_ = out;
+    }
+
+    // One level trained again from its snapshot, as the training loop runs it: candidate
+    // generation with the level seed, the split search (level-batched or per node) and routing of
+    // the samples into the next level's node-contiguous lists (into this trainer's buffers, which the
+    // snapshot never reads). best (host, [M]) receives the splits when not NULL.
+    void run_level(cf_level_snapshot* s, int mode, cf_split* best) {
+        cf_context* ctx = ds_->ctx;
+        make_current(ctx);
+        configure(s->C, s->cfg, mode);
+        const int F = static_cast<int>(cfg_.feature_count), T = cfg_.thresholds, M = s->M;
+        const long long n = s->n;
+        samples_[1].reserve(n);
+        snode_[1].reserve(n);
+        nodes_[1].reserve(2 * static_cast<size_t>(M));
+        hist_[1].reserve(2 * static_cast<size_t>(M) * C_);
+        splits_.reserve(M);
+        if (tree_.capacity < s->tree_next + 2 * M) tree_.reserve(s->tree_next + 2 * M, C_);
+        lf_.reserve(F, T);
+        cudaStream_t st = ctx->stream;
+        cudaEvent_t e0, e1;
+        CF_CUDA_CHECK(cudaEventCreate(&e0));
+        CF_CUDA_CHECK(cudaEventCreate(&e1));
+        struct Events {
+            cudaEvent_t a, b;
+            ~Events() {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } evs{e0, e1};
+        const DsView ds = view_of(ds_);
+        CF_CUDA_CHECK(cudaEventRecord(e0, st));
+        generate_level_features(ctx, ds, s->samples.get(), static_cast<uint32_t>(n), s->seed, cfg_.box_radius,
+                                cfg_.region_size, cfg_.use_depth_images, lf_);
+        if (mode == CF_TRAIN_PER_NODE) {
+            for (int i = 0; i < M; i++)
+                plain_.evaluate_node(ctx, ds, s->samples.get(), s->offsets[i], s->counts[i],
+                                     s->hist.get() + static_cast<size_t>(i) * C_, C_, lf_,
+                                     static_cast<int>(cfg_.max_samples_per_batch), splits_.get() + i, nullptr);
+        } else {
+            eval_.evaluate(ctx, ds, s->samples.get(), s->nodes.get(), s->hist.get(), M, s->counts, C_, lf_,
+                           splits_.get());
+        }
+        const bool scatter = s->level + 1 < cfg_.max_depth;
+        RouteResult rr = route_level(ctx, ds, s->samples.get(), s->snode.get(), n, s->nodes.get(), M, splits_.get(), lf_,
+                                     C_, s->level, static_cast<int>(cfg_.min_sample_count), s->tree_next, scatter,
+                                     tree_, rb_, scan_, samples_[1].get(), snode_[1].get(), nodes_[1].get(),
+                                     hist_[1].get());
+        CF_CUDA_CHECK(cudaEventRecord(e1, st));
+        CF_CUDA_CHECK(cudaEventSynchronize(e1));
+        if (rr.empty_child)
+            fail(CF_ERR_EMPTY_CHILD, "no samples in left or right node (level " + std::to_string(s->level) + ")");
+        CF_CUDA_CHECK(cudaEventElapsedTime(&s->last_ms, e0, e1));
+        s->last_evals = n * F;
+        s->next_nodes = rr.next_nodes;
+        s->next_samples = rr.next_samples;
+        if (best)
+            CF_CUDA_CHECK(cudaMemcpy(best, splits_.get(), sizeof(cf_split) * M, cudaMemcpyDeviceToHost));
+    }
+
     LevelEvaluator eval_;
 
 private:
+    cf_level_snapshot* snapshot(int cur, int level, int M, long long n, uint32_t seed, int tree_next,
+                                const std::vector<int>& counts, const std::vector<NodeDesc>& h_nodes) {
+        std::unique_ptr<cf_level_snapshot> s(new cf_level_snapshot());
+        s->ds = ds_;
+        s->level = level;
+        s->M = M;
+        s->C = C_;
+        s->n = n;
+        s->seed = seed;
+        s->tree_next = tree_next;
+        s->cfg = cfg_;
+        s->counts = counts;
+        s->offsets.resize(M + 1);
+        for (int i = 0; i < M; i++) s->offsets[i] = h_nodes[i].start;
+        s->offsets[M] = n;
+        s->samples.reserve(n);
+        s->snode.reserve(n);
+        s->nodes.reserve(M);
+        s->hist.reserve(static_cast<size_t>(M) * C_);
+        cudaStream_t st = ds_->ctx->stream;
+        CF_CUDA_CHECK(cudaMemcpyAsync(s->samples.get(), samples_[cur].get(), sizeof(Sample) * n, cudaMemcpyDeviceToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(s->snode.get(), snode_[cur].get(), sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(s->nodes.get(), nodes_[cur].get(), sizeof(NodeDesc) * M, cudaMemcpyDeviceToDevice, st));
+        CF_CUDA_CHECK(cudaMemcpyAsync(s->hist.get(), hist_[cur].get(), sizeof(uint32_t) * M * C_, cudaMemcpyDeviceToDevice,
+                                      st));
+        return s.release();
+    }
+
+    std::vector<int> capture_;
+    std::vector<cf_level_snapshot*>* captured_ = nullptr;
     cf_dataset* ds_;
     int C_;
     cf_train_config cfg_;
@@ -230,9 +353,8 @@ private:
     PlainNodeEvaluator plain_;
 };
 
-cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
-                    int32_t* seed_counter, int mode, const LevelEvaluator::Shard* shard) {
-    // the dataset keeps one trainer so its device buffers are allocated once, not per tree
+// The dataset's trainer (created on first use) holds the device buffers, allocated once, not per tree.
+TreeTrainer* acquire_trainer(cf_dataset* ds, int C, const cf_train_config& cfg, int mode) {
     if (ds->trainer == nullptr) {
         // the buffers of a destroyed dataset's trainer, if the context keeps some
         cf_context* ctx = ds->ctx;
@@ -249,7 +371,12 @@ cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, cons
         ds->trainer = new TreeTrainer(ds, C, cfg, mode);
         ds->trainer_free = [](void* p) { delete static_cast<TreeTrainer*>(p); };
     }
-    TreeTrainer* trainer = static_cast<TreeTrainer*>(ds->trainer);
+    return static_cast<TreeTrainer*>(ds->trainer);
+}
+
+cf_tree* train_tree(cf_dataset* ds, const cf_sample* samples, int N, int C, const cf_train_config& cfg, int tree_id,
+                    int32_t* seed_counter, int mode, const LevelEvaluator::Shard* shard) {
+    TreeTrainer* trainer = acquire_trainer(ds, C, cfg, mode);
     trainer->configure(C, cfg, mode);
     struct Reset {
         TreeTrainer* t;
@@ -525,6 +652,77 @@ cf_status cf_train_tree_sharded(cf_dataset* ds, int num_samples, const cf_sample
         *out = train_tree(ds, samples, num_samples, num_classes, *config, tree_id, seed_counter,
                           CF_TRAIN_LEVEL_BATCHED, &shard);
     });
+}
+
+cf_status cf_train_tree_snapshots(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                                  const cf_train_config* config, int tree_id, int32_t* seed_counter, int num_levels,
+                                  const int32_t* levels, cf_level_snapshot** snapshots, int* num_snapshots,
+                                  cf_tree** out) {
+    return guard([&] {
+        CF_REQUIRE(ds && samples && seed_counter && out && num_snapshots, "cf_train_tree_snapshots: NULL argument");
+        CF_REQUIRE(num_levels >= 0 && (num_levels == 0 || (levels && snapshots)),
+                   "cf_train_tree_snapshots: levels and snapshots are needed for num_levels > 0");
+        validate_config(config);
+        std::vector<int> want(levels, levels + num_levels);
+        for (int l : want) CF_REQUIRE(l >= 1, "cf_train_tree_snapshots: levels start at 1 (the root)");
+        std::vector<cf_level_snapshot*> got;
+        TreeTrainer* trainer = acquire_trainer(ds, num_classes, *config, CF_TRAIN_LEVEL_BATCHED);
+        struct Disarm {
+            TreeTrainer* t;
+            std::vector<cf_level_snapshot*>* got;
+            bool ok = false;
+            ~Disarm() {
+                t->capture({}, nullptr);
+                if (!ok)
+                    for (auto* p : *got) delete p;
+            }
+        } disarm{trainer, &got};
+        trainer->capture(want, &got);
+        *out = train_tree(ds, samples, num_samples, num_classes, *config, tree_id, seed_counter,
+                          CF_TRAIN_LEVEL_BATCHED, nullptr);
+        CF_CUDA_CHECK(cudaStreamSynchronize(ds->ctx->stream));
+        CF_REQUIRE(static_cast<int>(got.size()) <= num_levels, "cf_train_tree_snapshots: internal: too many levels");
+        for (size_t i = 0; i < got.size(); i++) snapshots[i] = got[i];
+        *num_snapshots = static_cast<int>(got.size());
+        disarm.ok = true;
+    });
+}
+
+cf_status cf_level_snapshot_info(cf_level_snapshot* s, int* level, int* num_nodes, int64_t* num_samples) {
+    return guard([&] {
+        CF_REQUIRE(s, "cf_level_snapshot_info: snapshot is NULL");
+        if (level) *level = s->level;
+        if (num_nodes) *num_nodes = s->M;
+        if (num_samples) *num_samples = s->n;
+    });
+}
+
+cf_status cf_level_snapshot_export(cf_level_snapshot* s, int64_t* node_offsets, cf_sample* samples, uint32_t* seed) {
+    return guard([&] {
+        CF_REQUIRE(s, "cf_level_snapshot_export: snapshot is NULL");
+        make_current(s->ds->ctx);
+        if (node_offsets) std::memcpy(node_offsets, s->offsets.data(), sizeof(int64_t) * (s->M + 1));
+        if (samples)
+            CF_CUDA_CHECK(cudaMemcpy(samples, s->samples.get(), sizeof(cf_sample) * s->n, cudaMemcpyDeviceToHost));
+        if (seed) *seed = s->seed;
+    });
+}
+
+cf_status cf_level_snapshot_run(cf_level_snapshot* s, int mode, cf_split* best, double* device_ms,
+                                int64_t* feature_evals, int* next_nodes, int64_t* next_samples) {
+    return guard([&] {
+        CF_REQUIRE(s && s->ds && s->ds->trainer, "cf_level_snapshot_run: snapshot or its dataset is gone");
+        CF_REQUIRE(mode == CF_TRAIN_LEVEL_BATCHED || mode == CF_TRAIN_PER_NODE, "cf_level_snapshot_run: unknown mode");
+        static_cast<TreeTrainer*>(s->ds->trainer)->run_level(s, mode, best);
+        if (device_ms) *device_ms = s->last_ms;
+        if (feature_evals) *feature_evals = s->last_evals;
+        if (next_nodes) *next_nodes = s->next_nodes;
+        if (next_samples) *next_samples = s->next_samples;
+    });
+}
+
+cf_status cf_level_snapshot_destroy(cf_level_snapshot* s) {
+    return guard([&] { delete s; });
 }
 
 cf_status cf_tree_info(cf_tree* tree, int* num_nodes, int* num_classes, int* depth, int* tree_id) {

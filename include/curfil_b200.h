@@ -233,9 +233,14 @@ cf_status cf_level_left_counts(cf_dataset* ds, int num_nodes, const int64_t* nod
  * (flip-Both samples counted twice), the feature table int8 [11][F], thresholds float [T][F] and
  * best [M]; node_offsets [M+1] is a HOST array. Scratch lives in one fixed 16 MiB device array
  * compiled into the library, so this call allocates nothing; limits: M <= 65536 nodes, at most 65536
- * work items, F <= 16384, F x T <= 2^20 (larger levels return CF_ERR_INVALID). The first call on a
- * device looks the array's device address up (make it before any stream capture). Calls share the
- * array: calls that overlap on the GPU (other threads or streams) race and must be serialised. */
+ * work items, F <= 16384, T <= 4096, F x T <= 2^20 (larger levels return CF_ERR_INVALID).
+ * Preconditions, checked on the device before the split search runs (CF_ERR_INVALID, nothing
+ * evaluated): every sample has image < num_images, x < width, y < height, flip <= 2 and a label
+ * < num_classes that its node's histogram counts; no threshold is NaN. The histograms should equal
+ * the nodes' class counts: other nonzero counts give meaningless scores but are not detected. The
+ * first call on a device loads the module that holds the array (make it before any stream capture).
+ * Calls share the array: calls that overlap on the GPU (other threads or streams) race and must be
+ * serialised. */
 cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const float* color, const int32_t* depth,
                                           int num_images, int width, int height, int num_nodes,
                                           const int64_t* node_offsets, const cf_sample* samples,
@@ -270,6 +275,35 @@ typedef int (*cf_allgather_fn)(const void* send, size_t bytes, void* recv, void*
 cf_status cf_train_tree_sharded(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
                                 const cf_train_config* config, int tree_id, int32_t* seed_counter, int rank,
                                 int world, cf_allgather_fn allgather, void* user, cf_tree** out);
+/* One level of a tree's training on its own. The reference trains a level as one pass of the loop
+ * body of RandomTreeTrain::train (random_tree.h:1262-1410): evaluateBestSplits for the level's open
+ * nodes (random_tree_image.cpp:239-502), then routing of every sample into its child. There it has
+ * no entry point of its own; here a level's input state (its node-contiguous samples, open nodes,
+ * node histograms and level seed) is captured during a training and can be trained again, to
+ * measure or compare the split search on a chosen level of a large tree without training the tree.
+ * cf_train_tree_snapshots trains like cf_train_tree (level-batched) and returns a snapshot of each
+ * listed level (root = 1) the tree reaches, in level order (*num_snapshots of them, at most
+ * num_levels). Snapshots keep device memory (about 20 bytes per sample) and use their dataset's
+ * training buffers: destroy them before the dataset. */
+typedef struct cf_level_snapshot cf_level_snapshot;
+cf_status cf_train_tree_snapshots(cf_dataset* ds, int num_samples, const cf_sample* samples, int num_classes,
+                                  const cf_train_config* config, int tree_id, int32_t* seed_counter, int num_levels,
+                                  const int32_t* levels, cf_level_snapshot** snapshots, int* num_snapshots,
+                                  cf_tree** out);
+cf_status cf_level_snapshot_info(cf_level_snapshot* snapshot, int* level, int* num_nodes, int64_t* num_samples);
+/* The level's node offsets [M + 1], samples [n] (host buffers, either may be NULL) and level seed:
+ * the inputs of evaluateBestSplits for this level (cf_generate_features with that seed gives the
+ * level's candidate table). */
+cf_status cf_level_snapshot_export(cf_level_snapshot* snapshot, int64_t* node_offsets, cf_sample* samples,
+                                   uint32_t* seed);
+/* Trains the level again as the training loop does: candidate generation, the split search in `mode`
+ * (CF_TRAIN_LEVEL_BATCHED or CF_TRAIN_PER_NODE) and routing into the next level's sample lists. best
+ * (host [M], may be NULL) receives the splits; device_ms is the level's time on the device (CUDA
+ * events), feature_evals = samples x features; next_nodes and next_samples describe the next level.
+ * Any pointer may be NULL. The snapshot itself is not changed, so runs repeat exactly. */
+cf_status cf_level_snapshot_run(cf_level_snapshot* snapshot, int mode, cf_split* best, double* device_ms,
+                                int64_t* feature_evals, int* next_nodes, int64_t* next_samples);
+cf_status cf_level_snapshot_destroy(cf_level_snapshot* snapshot);
 /* RandomForestImage::train (random_forest_image.cpp:132-182) on raw host frames: GPU integral images,
  * class-uniform sampling (random_tree_image.cpp:911-1059, one host thread), block sort, then
  * cf_train_tree per tree. labels uint8 [n][H][W]; ignored[C] marks ignoredColors. */

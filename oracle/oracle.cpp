@@ -969,3 +969,98 @@ int orc_sample_class_uniform_keys(int n, int width, int height, const uint8_t* l
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------------------------------
+ * Synthetic frames (the workloads' data, see oracle.h)
+ * ---------------------------------------------------------------------------------------- */
+namespace {
+
+/* SplitMix64 stream; uniform doubles from its top 53 bits, normals by Box-Muller. */
+class Mix64 {
+public:
+    explicit Mix64(uint64_t s) : state_(s) {}
+    uint64_t bits() {
+        state_ += 0x9E3779B97F4A7C15ull;
+        uint64_t z = state_;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double unit() { return static_cast<double>(bits() >> 11) * (1.0 / 9007199254740992.0); }
+    int index(int n) { return static_cast<int>(unit() * n); }
+    double gauss() {
+        const double a = std::max(unit(), 1e-300);
+        const double b = unit();
+        return std::sqrt(-2.0 * std::log(a)) * std::cos(6.283185307179586 * b);
+    }
+
+private:
+    uint64_t state_;
+};
+
+struct Cell {
+    double x, y, r, g, b, depth, slope_x, slope_y;
+    int cls;
+};
+
+void synthetic_frame(uint64_t seed, int frame, int W, int H, int K, int C, const double* class_rgb,
+                     const double* class_depth, uint8_t* rgb, uint16_t* depth, uint8_t* labels) {
+    Mix64 rng(seed * 0x100000001B3ull + static_cast<uint64_t>(frame) * 0x9E3779B97F4A7C15ull + 17);
+    std::vector<Cell> cells(K);
+    for (Cell& c : cells) {
+        c.x = rng.unit() * W;
+        c.y = rng.unit() * H;
+        c.cls = rng.index(C);
+        c.r = class_rgb[3 * c.cls + 0] + (rng.unit() - 0.5) * 30.0;
+        c.g = class_rgb[3 * c.cls + 1] + (rng.unit() - 0.5) * 30.0;
+        c.b = class_rgb[3 * c.cls + 2] + (rng.unit() - 0.5) * 30.0;
+        c.depth = class_depth[c.cls] + (rng.unit() - 0.5) * 600.0;
+        c.slope_x = (rng.unit() - 0.5) * 4.0;
+        c.slope_y = (rng.unit() - 0.5) * 4.0;
+    }
+    for (int y = 0; y < H; y++) {
+        for (int x = 0; x < W; x++) {
+            const Cell* near = &cells[0];
+            double best = 1e300;
+            for (const Cell& c : cells) {
+                const double d2 = (x - c.x) * (x - c.x) + (y - c.y) * (y - c.y);
+                if (d2 < best) {
+                    best = d2;
+                    near = &c;
+                }
+            }
+            const size_t p = static_cast<size_t>(y) * W + x;
+            const double base[3] = {near->r, near->g, near->b};
+            for (int k = 0; k < 3; k++) {
+                const double v = std::round(base[k] + 8.0 * rng.gauss());
+                rgb[3 * p + k] = static_cast<uint8_t>(std::min(255.0, std::max(0.0, v)));
+            }
+            const double plane = near->depth + near->slope_x * (x - near->x) + near->slope_y * (y - near->y);
+            const double clamped = std::min(5000.0, std::max(500.0, plane));
+            depth[p] = rng.unit() < 0.1 ? 0 : static_cast<uint16_t>(std::lround(clamped));
+            int label = near->cls;
+            if (C > 1 && rng.unit() < 0.05) {
+                const int other = rng.index(C - 1);
+                label = other >= label ? other + 1 : other;
+            }
+            labels[p] = static_cast<uint8_t>(label);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" void orc_synthetic_frames(uint64_t seed, int first, int n, int width, int height, int num_cells,
+                                     int num_classes, uint8_t* rgb, uint16_t* depth_mm, uint8_t* labels) {
+    Mix64 crng(seed ^ 0xC1A55E5ull);
+    std::vector<double> class_rgb(3 * num_classes), class_depth(num_classes);
+    for (int c = 0; c < num_classes; c++) {
+        for (int k = 0; k < 3; k++) class_rgb[3 * c + k] = 30.0 + 195.0 * crng.unit();
+        class_depth[c] = 900.0 + 3600.0 * crng.unit();
+    }
+    const size_t plane = static_cast<size_t>(width) * height;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < n; i++)
+        synthetic_frame(seed, first + i, width, height, num_cells, num_classes, class_rgb.data(), class_depth.data(),
+                        rgb + 3 * plane * i, depth_mm + plane * i, labels + plane * i);
+}

@@ -199,6 +199,17 @@ int orc_sample_class_uniform_keys(int n, int width, int height, const uint8_t* l
                                   int subsample_count, int* seed_counter, int capacity,
                                   orc_sample* out);
 
+/* The seeded synthetic RGB-D frames every workload here is made of (not a reference algorithm: the
+ * stand-in for recorded data). Per frame, from (seed, frame index): a Voronoi partition into
+ * num_cells cells, each taking a class with a class colour and depth shared by all frames; colour
+ * uint8 RGB = cell colour + N(0, 8^2) noise; depth uint16 mm = a plane per cell clamped to
+ * [500, 5000], 10% of pixels 0; labels = cell class with 5% flipped to another class. Frames
+ * first .. first + n - 1: rgb [n][H][W][3], depth [n][H][W], labels [n][H][W]. Restated here so that
+ * the CPU baseline needs nothing from the product library; a test pins it to the library's
+ * generator byte for byte. */
+void orc_synthetic_frames(uint64_t seed, int first, int n, int width, int height, int num_cells,
+                          int num_classes, uint8_t* rgb, uint16_t* depth_mm, uint8_t* labels);
+
 #ifdef __cplusplus
 }
 #endif

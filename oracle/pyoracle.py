@@ -337,3 +337,14 @@ def sample_class_uniform(labels, depth_mm, num_classes, ignore, subsample_count,
     if rc < 0:
         return rc, None, sc.value
     return rc, out[:rc].copy(), sc.value
+
+
+def synthetic_frames(seed, num_images, width, height, num_cells, num_classes, first=0):
+    """(rgb uint8 [n][H][W][3], depth uint16 [n][H][W], labels uint8 [n][H][W]) of the workloads'
+    seeded synthetic generator (restated here; frames first .. first + n - 1)."""
+    rgb = np.empty((num_images, height, width, 3), np.uint8)
+    depth = np.empty((num_images, height, width), np.uint16)
+    labels = np.empty((num_images, height, width), np.uint8)
+    lib().orc_synthetic_frames(ctypes.c_uint64(seed), first, num_images, width, height, num_cells, num_classes,
+                               _p(rgb), _p(depth), _p(labels))
+    return rgb, depth, labels

@@ -55,29 +55,42 @@ def random_features(rng, F, box_radius=60, region_size=15, depth_fraction=0.5):
     return f
 
 
-def compare_trees(gpu, ora, oracle_scores_ok=None, rel=1e-6):
-    """Node-by-node comparison of two breadth-first trees (dicts of arrays).
+def compare_trees(gpu, ora, rel=1e-6):
+    """Path-by-path comparison of two breadth-first trees (dicts of arrays).
 
-    Identical structure, split parameters, thresholds and histograms are required; a differing
-    split is accepted only where `oracle_scores_ok(node)` says the two choices tie within `rel`.
-    Returns the number of nodes compared before the first accepted divergence (or all).
+    Both trees are walked from the root together. At every pair of nodes reached by the same path the
+    histograms must be identical, and so must the split (leaf or not, feature parameters, threshold);
+    the score must agree to 1e-12. A differing split is accepted only where the two scores tie within
+    `rel` relative; the two subtrees below it then differ and are skipped, while every other subtree
+    is still compared. Returns the number of node pairs compared.
     """
-    n = min(len(gpu["left"]), len(ora["left"]))
-    for i in range(n):
-        np.testing.assert_array_equal(gpu["histogram"][i], ora["histogram"][i], err_msg="histogram of node %d" % i)
-        same = (gpu["left"][i] == ora["left"][i] and np.array_equal(gpu["feature"][i], ora["feature"][i]) and
-                (gpu["left"][i] < 0 or gpu["threshold"][i] == ora["threshold"][i]))
+    compared, skipped = 0, 0
+    stack = [(0, 0)]
+    while stack:
+        a, b = stack.pop()
+        np.testing.assert_array_equal(gpu["histogram"][a], ora["histogram"][b],
+                                      err_msg="histogram of node %d (oracle node %d)" % (a, b))
+        compared += 1
+        leaf_a, leaf_b = gpu["left"][a] < 0, ora["left"][b] < 0
+        assert leaf_a == leaf_b, "node %d / oracle node %d: leaf in one tree only" % (a, b)
+        if leaf_a:
+            continue
+        same = np.array_equal(gpu["feature"][a], ora["feature"][b]) and gpu["threshold"][a] == ora["threshold"][b]
         if not same:
-            if oracle_scores_ok is not None and oracle_scores_ok(i):
-                return i
-            raise AssertionError("node %d differs: gpu left=%d feat=%s thr=%r score=%r | oracle left=%d feat=%s "
-                                 "thr=%r score=%r" % (i, gpu["left"][i], gpu["feature"][i], gpu["threshold"][i],
-                                                      gpu["score"][i], ora["left"][i], ora["feature"][i],
-                                                      ora["threshold"][i], ora["score"][i]))
-        if gpu["left"][i] >= 0:
-            assert gpu["score"][i] == __import__("pytest").approx(ora["score"][i], rel=1e-12, abs=1e-14)
-    assert len(gpu["left"]) == len(ora["left"]), "node counts differ: %d vs %d" % (len(gpu["left"]), len(ora["left"]))
-    return n
+            if abs(gpu["score"][a] - ora["score"][b]) <= rel * abs(ora["score"][b]):
+                skipped += 1
+                continue
+            raise AssertionError("node %d differs: gpu feat=%s thr=%r score=%r | oracle node %d feat=%s thr=%r "
+                                 "score=%r" % (a, gpu["feature"][a], gpu["threshold"][a], gpu["score"][a], b,
+                                               ora["feature"][b], ora["threshold"][b], ora["score"][b]))
+        assert gpu["score"][a] == __import__("pytest").approx(ora["score"][b], rel=1e-12, abs=1e-14)
+        la, lb = int(gpu["left"][a]), int(ora["left"][b])
+        stack.append((la + 1, lb + 1))
+        stack.append((la, lb))
+    if skipped == 0:
+        assert len(gpu["left"]) == len(ora["left"]), "node counts differ: %d vs %d" % (len(gpu["left"]),
+                                                                                      len(ora["left"]))
+    return compared
 
 
 def oracle_tree_dict(t):

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import curfil_b200 as cf
+from oracle import pyoracle as orc
 from curfil_b200 import _build
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -66,6 +67,17 @@ def test_synthetic_frames_deterministic():
     tail = cf.synthetic_frames(7, 2, 64, 48, 12, 8, first=1)
     for x, y in zip(a, tail):
         np.testing.assert_array_equal(x[1:], y)
+
+
+@pytest.mark.parametrize("args", [(7, 3, 64, 48, 12, 8, 0), (2026, 1, 640, 480, 40, 40, 0), (5, 2, 80, 60, 10, 6, 3)])
+def test_oracle_generator_equals_library_generator(args):
+    """The CPU baseline makes its frames with the oracle's restatement of the generator; they must be
+    the library's frames byte for byte."""
+    seed, n, w, h, cells, classes, first = args
+    a = cf.synthetic_frames(seed, n, w, h, cells, classes, first=first)
+    b = orc.synthetic_frames(seed, n, w, h, cells, classes, first=first)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
 
 
 def small_tree(C=3):

@@ -57,5 +57,5 @@ def test_chunked_train_tree_matches_oracle(ctx, scene, flip):
     assert counter == ocounter
     g = tree.arrays()
     o = H.oracle_tree_dict(otree)
-    n = H.compare_trees(g, o, oracle_scores_ok=lambda i: abs(g["score"][i] - o["score"][i]) <= 1e-6 * o["score"][i])
+    n = H.compare_trees(g, o)
     assert n > 20

@@ -47,7 +47,7 @@ def test_train_tree_edges_match_oracle(ctx, scene, F, T, C, depth):
     assert counter == ocounter
     g = tree.arrays()
     o = H.oracle_tree_dict(otree)
-    H.compare_trees(g, o, oracle_scores_ok=lambda i: abs(g["score"][i] - o["score"][i]) <= 1e-6 * o["score"][i])
+    H.compare_trees(g, o)
     assert tree.num_nodes >= 3
 
 

@@ -252,7 +252,7 @@ def test_train_tree_matches_oracle(ctx, scene, flip):
     assert counter == ocounter
     g = tree.arrays()
     o = H.oracle_tree_dict(otree)
-    n = H.compare_trees(g, o, oracle_scores_ok=lambda i: abs(g["score"][i] - o["score"][i]) <= 1e-6 * o["score"][i])
+    n = H.compare_trees(g, o)
     assert n > 20
 
 
@@ -420,7 +420,7 @@ def test_forest_train_device_sampler_matches_oracle(ctx):
         assert rc == 0
         g = tree.arrays()
         o = H.oracle_tree_dict(ot)
-        H.compare_trees(g, o, oracle_scores_ok=lambda i: abs(g["score"][i] - o["score"][i]) <= 1e-6 * o["score"][i])
+        H.compare_trees(g, o)
 
 
 def test_forest_train_end_to_end_matches_oracle(ctx):
@@ -439,5 +439,5 @@ def test_forest_train_end_to_end_matches_oracle(ctx):
         assert rc == 0
         g = tree.arrays()
         o = H.oracle_tree_dict(ot)
-        H.compare_trees(g, o, oracle_scores_ok=lambda i: abs(g["score"][i] - o["score"][i]) <= 1e-6 * o["score"][i])
+        H.compare_trees(g, o)
         np.testing.assert_array_equal(tree.prior(), np.bincount(labels.ravel(), minlength=6))
