@@ -59,7 +59,7 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("max_batch_frames", ctypes.c_int32),
                 ("max_pending", ctypes.c_int32), ("pipeline_depth", ctypes.c_int32),
                 ("return_probabilities", ctypes.c_int32), ("policy", ctypes.c_int32), ("max_wait_ms", ctypes.c_float),
-                ("device_priority", ctypes.c_int32)]
+                ("device_priority", ctypes.c_int32), ("max_queue_ms", ctypes.c_float)]
 
 
 class EvalTuning(ctypes.Structure):
@@ -806,9 +806,10 @@ class Server:
     """cf_server: continuous-batching dense prediction on a resident forest."""
 
     def __init__(self, forest, hbm_budget_bytes=8 << 30, max_batch_frames=16, max_pending=4096, pipeline_depth=2,
-                 return_probabilities=False, policy=0, max_wait_ms=0.0, device_priority=0):
+                 return_probabilities=False, policy=0, max_wait_ms=0.0, device_priority=0, max_queue_ms=0.0):
         cfg = ServerConfig(int(hbm_budget_bytes), int(max_batch_frames), int(max_pending), int(pipeline_depth),
-                           int(return_probabilities), int(policy), float(max_wait_ms), int(device_priority))
+                           int(return_probabilities), int(policy), float(max_wait_ms), int(device_priority),
+                           float(max_queue_ms))
         h = _vp()
         _check(lib().cf_server_create(forest.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self.handle, self.forest = h, forest

@@ -113,6 +113,7 @@ struct cf_server {
     std::deque<std::shared_ptr<Request>> queue;
     std::unordered_map<int64_t, std::shared_ptr<Request>> requests;
     int64_t next_id = 1, submitted = 0, completed = 0, rejected = 0, batches = 0;
+    int64_t expired = 0;   // rejected after waiting longer than max_queue_ms
     bool stopping = false;
     std::thread launcher;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -145,10 +146,27 @@ struct cf_server {
                         break;
                     }
                 if (!slot) continue;
+                const double now = now_ms();
+                // load shedding: a request still queued max_queue_ms after its submission is refused
+                // instead of being served late (the queue is in arrival order, so expired requests are
+                // at its front)
+                if (cfg.max_queue_ms > 0.0f) {
+                    while (!queue.empty() && now - queue.front()->submit_ms > cfg.max_queue_ms) {
+                        auto& r = queue.front();
+                        r->status = CF_ERR_REJECTED;
+                        r->error = "request waited longer than max_queue_ms in the queue";
+                        r->done_ms = now;
+                        r->done = true;
+                        rejected++;
+                        expired++;
+                        queue.pop_front();
+                    }
+                    cv_done.notify_all();
+                    if (queue.empty()) continue;
+                }
                 // admission: frames in the policy's order (arrival, or smallest first with requests
                 // older than max_wait_ms ahead) while they fit in the slot's budget
                 size_t dev = 0, host = 0;
-                const double now = now_ms();
                 int level = -1;   // with device priorities a batch holds frames of one size class
                 while (!queue.empty() && static_cast<int>(batch.size()) < cfg.max_batch_frames) {
                     size_t pick = 0;
@@ -366,6 +384,7 @@ cf_status cf_server_create(cf_forest* forest, const cf_server_config* config, cf
                    "cf_server_create: policy is 0 (arrival order) or 1 (smallest first, max_wait_ms > 0)");
         CF_REQUIRE(config->device_priority == 0 || config->device_priority == 1,
                    "cf_server_create: device_priority is 0 or 1");
+        CF_REQUIRE(config->max_queue_ms >= 0.0f, "cf_server_create: max_queue_ms must be >= 0 (0: no limit)");
         cf_context* ctx = forest->ctx;
         make_current(ctx);
         std::unique_ptr<cf_server> s(new cf_server());

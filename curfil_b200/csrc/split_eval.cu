@@ -67,6 +67,21 @@ struct EvalArgs {
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Features of one histogram tile: as many as the budget holds for `cp` classes and T + 1 bins, at most
+// ft_max. With sample groups the lanes of a warp take (sample, feature) pairs in groups of a power of
+// two, so the tile is rounded down to one: 5 features would keep 3 of every 8 lanes idle, 4 keep all
+// 32 busy (the samples are read once more per tile, which costs far less).
+__host__ __device__ inline int tile_features(int budget, int cp, int T1, int ft_max, bool grouped) {
+    int ft = budget / (cp * T1);
+    ft = ft < 1 ? 1 : (ft > ft_max ? ft_max : ft);
+    if (grouped && ft < 32) {
+        int p = 1;
+        while (2 * p <= ft) p *= 2;
+        ft = p;
+    }
+    return ft;
+}
+
 // TP = stride of a feature's threshold row (T, or 32 for the padded search)
 struct SmemLayout {
     size_t counts, params, thr, rank, scores, bins, total;
@@ -202,8 +217,7 @@ level_eval_kernel(EvalArgs a) {
         const bool chunked = item.chunks > 1;
         const int N = chunked ? item.s_end - item.s_begin : nd.count;
         const long long sbase = nd.start + (chunked ? item.s_begin : 0);
-        int ft = a.bins_budget / (cp * T1);
-        ft = max(1, min(ft, a.ft_max));
+        const int ft = tile_features(a.bins_budget, cp, T1, a.ft_max, kGrouped);
 
         for (int f0 = item.f_begin; f0 < item.f_end; f0 += ft) {
             const int nf = min(ft, item.f_end - f0);
@@ -827,7 +841,8 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     level_eval_smem(C, T, tuning, &budget);
     // sample chunks of a node's items merge their counts on this device, so they are not sharded; a
     // chunked item covers at most the features of the smallest tile (all C classes present)
-    const int chunk_features = sharded ? 0 : std::max(1, std::min(tuning.ft_max, budget / (C * (T + 1))));
+    const int chunk_features =
+        sharded ? 0 : tile_features(budget, C, T + 1, tuning.ft_max, tuning.sample_groups != 0);
     int n_groups = 0;
     const int max_groups = static_cast<int>(kMaxChunkGroupBytes / (sizeof(uint32_t) * static_cast<size_t>(budget)));
     plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups,

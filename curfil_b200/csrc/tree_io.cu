@@ -11,7 +11,9 @@
 #include <unistd.h>
 #include <zlib.h>
 
+#include <algorithm>
 #include <cctype>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -274,6 +276,29 @@ private:
     std::string indent() const { return std::string(4 * depth_, ' '); }
 };
 
+// /proc/cpuinfo as "key: value" records, one per logical processor (the fields the reference's
+// header keys numPhysicalCPUs and processorModels are taken from, export.cpp:91-177).
+std::vector<std::map<std::string, std::string>> cpu_records() {
+    std::vector<std::map<std::string, std::string>> recs;
+    FILE* f = std::fopen("/proc/cpuinfo", "r");
+    if (!f) return recs;
+    auto trim = [](const std::string& v) {
+        const size_t a = v.find_first_not_of(" \t\r\n"), b = v.find_last_not_of(" \t\r\n");
+        return a == std::string::npos ? std::string() : v.substr(a, b - a + 1);
+    };
+    char line[4096];
+    while (std::fgets(line, sizeof line, f)) {
+        const std::string l(line);
+        const size_t colon = l.find(':');
+        if (colon == std::string::npos) continue;
+        const std::string k = trim(l.substr(0, colon)), v = trim(l.substr(colon + 1));
+        if (k == "processor" || recs.empty()) recs.emplace_back();   // "processor" opens a record
+        if (!v.empty()) recs.back()[k] = v;
+    }
+    std::fclose(f);
+    return recs;
+}
+
 const char* mode_string(int m) { return m == 0 ? "cpu" : (m == 2 ? "compare" : "gpu"); }
 int parse_mode(const std::string& s) {
     if (s == "cpu") return 0;
@@ -350,6 +375,21 @@ cf_status cf_tree_write_json(cf_tree* tree, const cf_train_config* config, const
         w.kv("date", date);
         w.kv("randomSeed", std::to_string(config->random_seed));
         w.kv("folderTraining", "");
+        // host description keys of the reference header (export.cpp:198-200)
+        const auto cpus = cpu_records();
+        int physical = 0;
+        std::vector<std::string> models;
+        for (const auto& r : cpus) {
+            auto it = r.find("physical id");
+            if (it != r.end()) physical = std::max(physical, std::atoi(it->second.c_str()) + 1);
+            it = r.find("model name");
+            if (it != r.end() && std::find(models.begin(), models.end(), it->second) == models.end())
+                models.push_back(it->second);
+        }
+        std::sort(models.begin(), models.end());
+        w.kv("numCores", std::to_string(std::max(1L, sysconf(_SC_NPROCESSORS_ONLN))));
+        w.kv("numPhysicalCPUs", std::to_string(physical));
+        w.array("processorModels", models);
         w.kv("accelerationMode", mode_string(config->acceleration_mode));
         w.array("deviceId", {"0"});
         w.kv("samplesPerImage", std::to_string(config->samples_per_image));
@@ -432,6 +472,7 @@ cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t*
         // breadth-first walk: node index = id - treeId
         std::vector<const Json*> queue{&tj};
         std::vector<int> index{0};
+        std::vector<char> seen;   // node indices read (levels may start at 0 in hand-built files)
         int count = 0;
         t->resize(0);
         for (size_t q = 0; q < queue.size(); q++) {
@@ -440,7 +481,10 @@ cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t*
             if (i + 1 > count) {
                 count = i + 1;
                 t->resize(count);
+                seen.resize(count, 0);
             }
+            if (seen[i]) fail(CF_ERR_IO, "tree file: node id " + std::to_string(i + t->tree_id) + " appears twice");
+            seen[i] = 1;
             read_node(j, t->tree_id, *t, 0, i);
             const Json* l = j.get("left");
             const Json* r = j.get("right");
@@ -478,7 +522,7 @@ cf_status cf_tree_read_json(const char* path, cf_train_config* config, uint32_t*
         }
         // every index must have been filled
         for (int i = 0; i < count; i++)
-            if (t->level[i] == 0) fail(CF_ERR_IO, "tree file: missing node " + std::to_string(i));
+            if (!seen[i]) fail(CF_ERR_IO, "tree file: missing node " + std::to_string(i));
         // re-apply splits (resize during the walk may have reset nothing; values were written in place)
         *out = t.release();
     });

@@ -429,6 +429,9 @@ typedef struct cf_server_config {
                                    and runs on a stream whose CUDA priority rises as the class's frames get
                                    smaller, so the thread blocks of small frames are scheduled ahead of those
                                    still waiting in a larger frame's launch; 0: one priority for all */
+    float max_queue_ms;         /* load shedding: a request still queued this long after its submission is
+                                   refused (cf_server_wait returns CF_ERR_REJECTED) instead of being served
+                                   late; 0: no limit */
 } cf_server_config;
 
 typedef struct cf_request_stats {

@@ -182,3 +182,45 @@ def test_normalize_histogram_entry_point_kats(kat):
 def test_normalize_histogram_rejects_empty_prior():
     with pytest.raises(cf.CurfilError):
         cf.normalize_histogram([1, 2], [0, 0])
+
+
+def test_reads_a_tree_file_laid_out_as_the_reference_writes_it(tmp_path):
+    """A gzip JSON file with the reference's header keys (numCores, numPhysicalCPUs, processorModels,
+    deviceId, ...) and node layout (export.cpp:180-290) holding the recall tree of
+    random_tree_image_gpu_test.cu:990-1130 is read back exactly."""
+    from tests.golden import reference_kats as K
+    from tests.golden import reference_tree_file as R
+    path = tmp_path / "tree0.json.gz"
+    R.write(path)
+    t, cfg, prior = cf.Tree.read_json(path)
+    a = t.arrays()
+    np.testing.assert_array_equal(a["left"], [1, 3, -1, -1, -1])
+    np.testing.assert_array_equal(a["level"], [0, 1, 1, 2, 2])
+    np.testing.assert_array_equal(a["feature"][0], K.RECALL_TREE["split2"]["feature"])
+    np.testing.assert_array_equal(a["feature"][1], K.RECALL_TREE["split1"]["feature"])
+    assert a["threshold"][0] == np.float32(K.RECALL_TREE["split2"]["threshold"])
+    assert a["threshold"][1] == np.float32(K.RECALL_TREE["split1"]["threshold"])
+    assert a["score"][0] == K.RECALL_TREE["split2"]["score"] and a["score"][1] == K.RECALL_TREE["split1"]["score"]
+    np.testing.assert_array_equal(a["feature_id"][:2], [2, 1])
+    for i in (1, 2, 3, 4):
+        np.testing.assert_array_equal(a["histogram"][i], K.RECALL_TREE["hist"][i])
+    np.testing.assert_array_equal(a["num_samples"], [170, 30, 140, 30, 70])
+    np.testing.assert_array_equal(prior, K.RECALL_TREE["prior"])
+    assert (cfg.random_seed, cfg.samples_per_image, cfg.feature_count, cfg.thresholds, cfg.max_depth) == \
+        (4711, 100, 1000, 50, 15)
+    assert (cfg.box_radius, cfg.region_size, cfg.min_sample_count, cfg.max_samples_per_batch) == (127, 50, 32, 100000)
+    assert (cfg.num_threads, cfg.max_images, cfg.image_cache_size, cfg.acceleration_mode) == (1, 5, 5, 2)
+    assert (cfg.use_cie_lab, cfg.use_depth_filling, cfg.use_depth_images, cfg.subsampling_type) == (1, 0, 1, 0)
+    # written back by the library: the reference's header keys in the reference's order
+    import gzip
+    import json
+    out = tmp_path / "again.json.gz"
+    t.write_json(out, cfg, prior=prior)
+    doc = json.loads(gzip.open(out).read().decode())
+    assert list(doc.keys()) == R.HEADER_KEYS
+    assert int(doc["numCores"]) >= 1 and int(doc["numPhysicalCPUs"]) >= 0
+    assert isinstance(doc["processorModels"], list) and doc["deviceId"] == ["0"]
+    t2, _, _ = cf.Tree.read_json(out)
+    b = t2.arrays()
+    for k in ("level", "left", "feature", "threshold", "feature_id", "histogram", "num_samples"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)

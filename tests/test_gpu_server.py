@@ -148,3 +148,32 @@ def test_device_priority_streams_same_results(forest):
     server.close()
     with pytest.raises(cf.CurfilError):
         cf.Server(forest, device_priority=2)
+
+
+def test_overload_sheds_requests_that_wait_too_long(forest):
+    """With max_queue_ms a request still queued that long after its submission is refused
+    (CF_ERR_REJECTED) instead of served late; every served frame is still the frame served alone,
+    and no served frame waited in the queue longer than the limit."""
+    rgb, depth, _ = cf.synthetic_frames(600, 1, 1280, 960, 12, 10)
+    alone = cf.Server(forest, hbm_budget_bytes=1 << 30, max_batch_frames=1, pipeline_depth=1)
+    ref = alone.wait(alone.submit(rgb[0], depth[0]), depth[0].shape)[0]
+    alone.close()
+    server = cf.Server(forest, hbm_budget_bytes=1 << 30, max_batch_frames=1, pipeline_depth=1, max_queue_ms=1.0)
+    ids = [server.submit(rgb[0], depth[0]) for _ in range(40)]   # a burst far beyond one slot's pace
+    served, refused = 0, 0
+    for rid in ids:
+        try:
+            labels, _, st = server.wait(rid, depth[0].shape)
+        except cf.CurfilError as e:
+            assert e.status == 7 and "max_queue_ms" in str(e)
+            refused += 1
+            continue
+        served += 1
+        np.testing.assert_array_equal(labels, ref)
+        assert st.admitted_ms - st.submit_ms <= 1.0 + 0.5   # the limit, plus the launcher's own latency
+    c = server.counters()
+    assert served >= 1 and refused >= 1 and served + refused == 40
+    assert c["rejected"] == refused and c["completed"] == served
+    server.close()
+    with pytest.raises(cf.CurfilError):
+        cf.Server(forest, max_queue_ms=-1.0)
