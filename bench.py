@@ -127,6 +127,7 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.times = []
 
     def __enter__(self):
         try:
@@ -142,6 +143,20 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.times.append(time.perf_counter())
+
+    def between(self, t0, t1):
+        """(median SM MHz, fraction of samples with sw_power_cap active) of the samples read in [t0, t1]."""
+        sm, cap = [], []
+        for t, ln in zip(self.times, self.lines):
+            parts = [p.strip() for p in ln.split(",")]
+            if t0 <= t <= t1 and len(parts) >= 9:
+                try:
+                    sm.append(float(parts[1]))
+                except ValueError:
+                    continue
+                cap.append(parts[8].lower() == "active")
+        return (statistics.median(sm) if sm else None), (sum(cap) / len(cap) if cap else None)
 
     def __exit__(self, *a):
         if self.proc:
@@ -315,15 +330,27 @@ def headline(ctx, stream, local, rank, world, args, barrier, max_over_ranks, sum
                                                     cf.forest_seed(cfg.random_seed) + tree_id, ctx=ctx)
     del rgb, labels
     setup_s = time.perf_counter() - t0
-    tree, snaps, _ = cf.train_tree_snapshots(ds, samples, C3["classes"], cfg, LEVELS, tree_id=tree_id,
-                                             seed_counter=counter)
+    with ClockSampler(local) as tclk:
+        time.sleep(0.5)
+        t_call = time.perf_counter()
+        tree, snaps, _ = cf.train_tree_snapshots(ds, samples, C3["classes"], cfg, LEVELS, tree_id=tree_id,
+                                                 seed_counter=counter)
     ev, dev_ms, nlev = tree.train_stats()
+    # each level's time beside the SM clock and power-cap samples taken while it ran (the level's start
+    # is known on the device timeline; the training's first device work follows the call by the
+    # samples' upload, a few ms)
+    levels_ms = []
+    for (n_, s_, ms_), st in zip(tree.level_stats(), tree.level_starts()):
+        mhz, capped = tclk.between(t_call + st / 1e3, t_call + (st + ms_) / 1e3)
+        levels_ms.append([n_, s_, round(ms_, 1), mhz, None if capped is None else round(capped, 2)])
     out["tree"] = {"tree_id": tree_id, "nodes": tree.num_nodes, "depth": tree.depth, "levels": nlev,
                    "samples": len(samples), "device_ms": dev_ms, "feature_evals": ev,
                    "feature_evals_per_s": ev / (dev_ms / 1e3),
                    "note": "the whole tree trained once (level-batched) while the snapshots were taken; "
                            "setup (frames, upload, integral images, device sampling) %.1f s" % setup_s,
-                   "levels_ms": [[n, s, round(ms, 1)] for n, s, ms in tree.level_stats()]}
+                   "levels_ms": levels_ms,
+                   "levels_ms_columns": ["open nodes", "samples", "split search ms", "median SM MHz while it ran",
+                                         "fraction of clock samples with sw_power_cap active"]}
     tree.close()
     assert [s.level for s in snaps] == list(LEVELS), "the tree did not reach every benchmarked level"
 
@@ -568,7 +595,7 @@ def config1(ctx, stream):
     # prediction of the held-out frames: GPU from host frames vs the oracle (the reference's CPU predict)
     forest = cf.Forest(ctx, [tree], prior=prior)
     hr, hd = rgb[n:], depth[n:]
-    forest.predict(hr[:1], hd[:1])
+    forest.predict(hr, hd)
     t0 = time.perf_counter()
     probs, lab = forest.predict(hr, hd)
     gpu_s = time.perf_counter() - t0

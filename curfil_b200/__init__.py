@@ -393,6 +393,13 @@ class Tree:
         _check(lib().cf_tree_level_stats(self.handle, n.value, ctypes.byref(n), _p(nodes), _p(samples), _p(ms)))
         return list(zip(nodes.tolist(), samples.tolist(), ms.tolist()))
 
+    def level_starts(self):
+        """Start of each level's split search, ms after the training's first device work."""
+        n = len(self.level_stats())
+        out = np.zeros(n, np.float32)
+        _check(lib().cf_tree_level_starts(self.handle, n, _p(out)))
+        return out.tolist()
+
     def train_stats(self):
         ev, ms, lv = ctypes.c_int64(), ctypes.c_double(), _i32()
         _check(lib().cf_tree_train_stats(self.handle, ctypes.byref(ev), ctypes.byref(ms), ctypes.byref(lv)))

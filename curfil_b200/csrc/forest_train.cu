@@ -165,9 +165,12 @@ std::vector<cf_sample> sample_tree(int num_images, int width, int height, const 
     const int subsample = static_cast<int>(config.samples_per_image / static_cast<uint32_t>(num_trees));
     CF_REQUIRE(subsample > 0, "samplesPerImage / treeCount must be > 0");
     const uint8_t flip = config.horizontal_flipping ? 2 : 0;
-    if (frames && config.sampler == 1 && config.subsampling_type == 0) {
-        std::vector<cf_sample> samples = sample_class_uniform_device(ctx, *frames, images, depth_mm, num_classes,
-                                                                     ignored, subsample, rs, flip, &prior);
+    if (frames && config.sampler == 1) {
+        std::vector<cf_sample> samples =
+            config.subsampling_type == 0
+                ? sample_class_uniform_device(ctx, *frames, images, depth_mm, num_classes, ignored, subsample, rs, flip,
+                                              &prior)
+                : sample_pixel_uniform_device(ctx, *frames, images, num_classes, ignored, subsample, rs, flip, &prior);
         for (auto& s : samples) s.image = static_cast<uint32_t>(images[s.image]);
         return samples;
     }
@@ -235,7 +238,8 @@ cf_status cf_sample_tree_pixels_device(cf_context* ctx, int num_images, int widt
         CF_REQUIRE(num_images >= 1 && width >= 1 && height >= 1, "cf_sample_tree_pixels_device: empty input");
         CF_REQUIRE(num_classes >= 1 && num_classes <= 256, "cf_sample_tree_pixels_device: classes must be in [1, 256]");
         CF_REQUIRE(num_trees >= 1, "cf_sample_tree_pixels_device: need at least one tree");
-        CF_REQUIRE(config->subsampling_type == 0, "cf_sample_tree_pixels_device: classUniform sampling only");
+        CF_REQUIRE(config->subsampling_type == 0 || config->subsampling_type == 1,
+                   "cf_sample_tree_pixels_device: unknown subsamplingType");
         make_current(ctx);
         DeviceFrames frames;
         frames.upload(ctx, num_images, width, height, labels, depth_mm);
@@ -292,7 +296,7 @@ cf_status cf_forest_train(cf_context* ctx, int num_images, int width, int height
         }
         CF_REQUIRE(config->sampler == 0 || config->sampler == 1, "unknown sampler");
         std::unique_ptr<DeviceFrames> frames;
-        if (config->sampler == 1 && config->subsampling_type == 0) {
+        if (config->sampler == 1) {
             frames.reset(new DeviceFrames());
             frames->upload(ctx, num_images, width, height, labels, depth_mm);
         }

@@ -151,8 +151,10 @@ struct cf_context {
     // measured on B200 with 200 frames 640x480, 40 classes, 2000 features x 20 thresholds: a 28 KB
     // histogram leaves ~140 KB of the SM's unified memory to L1 for the integral-image gathers, and
     // ~64 items per CTA slot keep the last wave of a level short; sample groups without increment
-    // aggregation were 8 % faster than thread-per-sample with aggregation
-    static cf_eval_tuning default_tuning() { return cf_eval_tuning{32, 7168, 0, 3, 8, 64.0f, 1}; }
+    // aggregation were 8 % faster than thread-per-sample with aggregation. With 1000 frames and
+    // 4000 features x 32 thresholds, tiles of at most 16 features (shared staging sized for 16, not
+    // 32) left more L1 and were 3-12 % faster per level.
+    static cf_eval_tuning default_tuning() { return cf_eval_tuning{16, 7168, 0, 3, 8, 64.0f, 1}; }
     std::mutex mu;
     struct KernelEvents {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;

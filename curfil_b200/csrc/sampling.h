@@ -22,6 +22,11 @@ struct DeviceFrames {
     DevArray<int> bad;
     DevArray<unsigned long long> cut, count;
     DevArray<uint4> candidates;
+    // selection and ordering on the device (radix sorts)
+    DevArray<uint32_t> idx_a, idx_b, class_count, class_start;
+    DevArray<unsigned long long> key_a, key_b;
+    DevArray<uint8_t> sort_temp;
+    DevArray<cf_sample> out;
 
     DeviceFrames() = default;
     DeviceFrames(const DeviceFrames&) = delete;
@@ -40,5 +45,13 @@ std::vector<cf_sample> sample_class_uniform_device(cf_context* ctx, DeviceFrames
                                                    const std::vector<int>& images, const uint16_t* depth_host,
                                                    int C, const uint8_t* ignored, int subsample_count,
                                                    RandomSource& rs, uint8_t flip, std::vector<uint32_t>* prior);
+
+// pixelUniform samples of the listed images in the reference's definition (its random streams: the
+// image of each sample from one Sampler, its pixel from two fresh Samplers, redrawn while the label is
+// ignored), drawn on the device, block-sorted as RandomTreeImage::train sorts them; image field =
+// position in `images`. Advances `rs` as the reference does (1 + 2 x samples seeds).
+std::vector<cf_sample> sample_pixel_uniform_device(cf_context* ctx, DeviceFrames& frames, const std::vector<int>& images,
+                                                   int C, const uint8_t* ignored, int subsample_count, RandomSource& rs,
+                                                   uint8_t flip, std::vector<uint32_t>* prior);
 
 }  // namespace cf

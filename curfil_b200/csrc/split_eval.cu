@@ -683,6 +683,11 @@ __global__ void plain_score_kernel(const uint32_t* __restrict__ counters, const 
 // Shared-memory layout of a level_eval launch; budget = histogram words (at least one feature).
 SmemLayout level_eval_smem(int C, int T, const EvalTuning& tuning, int* budget) {
     *budget = std::max(tuning.bins_budget_words, C * (T + 1));
+    // with sample groups a tile holds a power-of-two number of features: the budget is trimmed to the
+    // largest such tile for all C classes, so no shared memory is reserved that no tile of a node
+    // with every class present would use (what is left stays L1); nodes with fewer classes fit the
+    // same or more features in it
+    if (tuning.sample_groups) *budget = tile_features(*budget, C, T + 1, tuning.ft_max, true) * C * (T + 1);
     const int TP = padded_row(T) ? padded_row(T) : T;
     return SmemLayout(C, T, TP + 1, tuning.ft_max, *budget);   // rows skewed by one bank with sample groups
 }
@@ -782,6 +787,9 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
     // sample chunks where the level has too few items to fill the resident CTAs
     const long long want = static_cast<long long>(kChunkItemsPerSlot) * slots;
     const int k = chunk_features > 0 && plain_items < want ? static_cast<int>((want + plain_items - 1) / plain_items) : 1;
+    // nodes of at least kChunkBigNodeSamples are cut into slices as well, however many items the level
+    // has: their sweeps then share the frames of one slice in L2 instead of each CTA streaming a node
+    // of frames from DRAM on its own (bounded by the groups' memory, max_groups)
     int groups = 0;
     items.clear();
     range.assign(M + 1, 0);
@@ -789,6 +797,10 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
     for (int n = 0; n < M; n++) {
         range[n] = static_cast<int>(items.size());
         int chunks = std::min(k, node_counts[n] / kMinChunkSamples);
+        if (chunk_features > 0 && node_counts[n] >= kChunkBigNodeSamples) chunks = std::max(chunks, 2);
+        if (chunks > 1)   // slices of about kChunkTargetSamples, for the L2 locality of a chunk-major queue
+            chunks = std::min(std::max(chunks, (node_counts[n] + kChunkTargetSamples - 1) / kChunkTargetSamples),
+                              node_counts[n] / kMinChunkSamples);
         if (chunks > 1) {
             const int node_groups = (F + std::min(per[n], chunk_features) - 1) / std::min(per[n], chunk_features);
             if (groups + node_groups > max_groups) chunks = 1;   // over the group memory limit: whole-node items
@@ -803,7 +815,7 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
             it.s_begin = 0;
             it.s_end = node_counts[n];
             it.group = -1;
-            it.pad = 0;
+            it.chunk = 0;
             if (chunks <= 1) {
                 items.push_back(it);
                 work.push_back(static_cast<long long>(node_counts[n]) * (it.f_end - it.f_begin));
@@ -811,6 +823,7 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
             }
             it.group = groups++;
             for (int c = 0; c < chunks; c++) {
+                it.chunk = c;
                 it.s_begin = static_cast<int>(static_cast<long long>(node_counts[n]) * c / chunks);
                 it.s_end = static_cast<int>(static_cast<long long>(node_counts[n]) * (c + 1) / chunks);
                 items.push_back(it);
@@ -823,7 +836,14 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
     const int n_items = static_cast<int>(items.size());
     order.resize(n_items);
     for (int i = 0; i < n_items; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+    // chunked items first, chunk-major (by slice, then group: slice c of every node covers about the
+    // same frames, since a node's samples are ordered by frame); then the rest, largest first
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const bool cx = items[x].chunks > 1, cy = items[y].chunks > 1;
+        if (cx != cy) return cx;
+        if (cx) return items[x].chunk != items[y].chunk ? items[x].chunk < items[y].chunk : items[x].group < items[y].group;
+        return work[x] > work[y];
+    });
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -24,7 +24,7 @@ struct EvalItem {
     int s_begin;
     int s_end;
     int group;
-    int pad;
+    int chunk;   // position of this item's slice among its group's chunks (0 for whole-node items)
 };
 
 constexpr int kMaxCand = 4;
@@ -45,7 +45,7 @@ struct ItemCandidates {
 
 // Launch shape of level_eval (cf_eval_tuning of the context; 256 threads per CTA).
 struct EvalTuning {
-    int ft_max = 32;              // features per tile upper bound
+    int ft_max = 16;              // features per tile upper bound
     int bins_budget_words = 7168;   // shared-memory histogram budget per CTA (u32 words)
     int warp_aggregate = 1;       // __match_any_sync aggregation of the shared-memory increments
     int ctas_per_sm = 3;
@@ -62,10 +62,16 @@ struct EvalTuning {
 // where one or a few nodes hold every sample), the items of nodes with at least 2 x kMinChunkSamples
 // samples cover at most chunk_features features (one histogram tile) and are cut into sample chunks,
 // for at most max_groups groups (nodes past the limit keep whole-node items); *n_groups receives the
-// number of chunk groups.
+// number of chunk groups. Chunked items come first in the order, chunk-major.
 constexpr int kChunkItemsPerSlot = 4;
 constexpr int kMinChunkSamples = 4096;
-constexpr size_t kMaxChunkGroupBytes = size_t(64) << 20;   // merged histograms of one level's chunk groups
+// Samples per chunk where a level is chunked: about eight frames' worth at 8000 samples per frame,
+// whose integral images (6 MB per 640x480 frame) fit in L2 together. Chunked items are queued
+// chunk-major (every group's first chunk, then every group's second, ...), so the resident CTAs all
+// gather from the same few frames and the gathers hit L2 instead of DRAM.
+constexpr int kChunkTargetSamples = 65536;
+constexpr size_t kMaxChunkGroupBytes = size_t(512) << 20;   // merged histograms of one level's chunk groups
+constexpr int kChunkBigNodeSamples = 4 * 65536;             // nodes this large are always cut into slices
 void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuning& tuning, int slots,
                       std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
                       int chunk_features = 0, int* n_groups = nullptr, int max_groups = 0);

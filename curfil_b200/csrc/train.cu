@@ -205,7 +205,6 @@ public:
         CF_CUDA_CHECK(cudaEventSynchronize(ev1));
         float ms = 0;
         CF_CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
-        cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
 
         auto* t = new cf_tree();
@@ -233,9 +232,13 @@ public:
             float lms = 0;
             cudaEventElapsedTime(&lms, pr.first, pr.second);
             t->level_eval_ms.push_back(lms);
+            float start = 0;
+            cudaEventElapsedTime(&start, ev0, pr.first);
+            t->level_start_ms.push_back(start);
             cudaEventDestroy(pr.first);
             cudaEventDestroy(pr.second);
         }
+        cudaEventDestroy(ev0);
         return t;
     }
 
@@ -304,6 +307,15 @@ public:
     }
 
     LevelEvaluator eval_;
+    // device buffers of the host-buffer entry points (evaluateBestSplits, candidate generation), kept
+    // so that repeated calls on a dataset do not allocate and free their inputs each time
+    struct HostCall {
+        DevArray<Sample> samples;
+        DevArray<NodeDesc> nodes;
+        DevArray<uint32_t> hist;
+        DevArray<cf_split> best;
+        LevelFeatures lf;
+    } host_;
 
 private:
     cf_level_snapshot* snapshot(int cur, int level, int M, long long n, uint32_t seed, int tree_next,
@@ -523,11 +535,12 @@ cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample*
         cf_context* ctx = ds->ctx;
         make_current(ctx);
         validate_samples(ds, samples, num_samples, 256);
-        Uploaded u;
-        upload_samples(ctx, u.samples, samples, num_samples);
-        LevelFeatures lf;
+        TreeTrainer* tr = acquire_trainer(ds, 1, cf_train_config{}, CF_TRAIN_LEVEL_BATCHED);
+        TreeTrainer::HostCall& hc = tr->host_;
+        upload_samples(ctx, hc.samples, samples, num_samples);
+        LevelFeatures& lf = hc.lf;
         lf.reserve(num_features, num_thresholds);
-        generate_level_features(ctx, view_of(ds), u.samples.get(), static_cast<uint32_t>(num_samples), seed, box_radius,
+        generate_level_features(ctx, view_of(ds), hc.samples.get(), static_cast<uint32_t>(num_samples), seed, box_radius,
                                 region_size, use_depth_images, lf);
         CF_CUDA_CHECK(cudaMemcpyAsync(features, lf.feat.get(), 11 * static_cast<size_t>(num_features),
                                       cudaMemcpyDeviceToHost, ctx->stream));
@@ -566,11 +579,12 @@ void evaluate_level_host(cf_dataset* ds, int num_nodes, const int64_t* node_offs
             for (long long s = node_offsets[i]; s < node_offsets[i + 1]; s++)
                 hist[static_cast<size_t>(i) * num_classes + samples[s].label] += samples[s].flip == 2 ? 2 : 1;
         }
-        Uploaded u;
-        upload_samples(ctx, u.samples, samples, n);
-        DevArray<NodeDesc> d_nodes;
-        DevArray<uint32_t> d_hist;
-        DevArray<cf_split> d_best;
+        TreeTrainer* tr = acquire_trainer(ds, num_classes, cf_train_config{}, CF_TRAIN_LEVEL_BATCHED);
+        TreeTrainer::HostCall& hc = tr->host_;
+        upload_samples(ctx, hc.samples, samples, n);
+        DevArray<NodeDesc>& d_nodes = hc.nodes;
+        DevArray<uint32_t>& d_hist = hc.hist;
+        DevArray<cf_split>& d_best = hc.best;
         d_nodes.reserve(num_nodes);
         d_hist.reserve(hist.size());
         d_best.reserve(num_nodes);
@@ -578,22 +592,22 @@ void evaluate_level_host(cf_dataset* ds, int num_nodes, const int64_t* node_offs
                                       ctx->stream));
         CF_CUDA_CHECK(cudaMemcpyAsync(d_hist.get(), hist.data(), sizeof(uint32_t) * hist.size(), cudaMemcpyHostToDevice,
                                       ctx->stream));
-        LevelFeatures lf;
+        LevelFeatures& lf = hc.lf;
         lf.reserve(num_features, num_thresholds);
         CF_CUDA_CHECK(cudaMemcpyAsync(lf.feat.get(), features, 11 * static_cast<size_t>(num_features),
                                       cudaMemcpyHostToDevice, ctx->stream));
         CF_CUDA_CHECK(cudaMemcpyAsync(lf.thr.get(), thresholds, sizeof(float) * num_features * num_thresholds,
                                       cudaMemcpyHostToDevice, ctx->stream));
         prepare_eval_features(ctx, lf);
-        LevelEvaluator ev;
+        LevelEvaluator& ev = tr->eval_;
         DevArray<uint32_t> d_left;
         const size_t n_left = static_cast<size_t>(num_nodes) * num_features * num_thresholds * num_classes;
         if (left_counts) {
             d_left.reserve(n_left);
             CF_CUDA_CHECK(cudaMemsetAsync(d_left.get(), 0, sizeof(uint32_t) * n_left, ctx->stream));
         }
-        ev.evaluate(ctx, view_of(ds), u.samples.get(), d_nodes.get(), d_hist.get(), num_nodes, counts, num_classes, lf,
-                    d_best.get(), left_counts ? d_left.get() : nullptr);
+        ev.evaluate(ctx, view_of(ds), hc.samples.get(), d_nodes.get(), d_hist.get(), num_nodes, counts, num_classes,
+                    lf, d_best.get(), left_counts ? d_left.get() : nullptr);
         CF_CUDA_CHECK(cudaMemcpyAsync(best, d_best.get(), sizeof(cf_split) * num_nodes, cudaMemcpyDeviceToHost,
                                       ctx->stream));
         if (left_counts)
@@ -805,6 +819,14 @@ cf_status cf_tree_level_stats(cf_tree* tree, int capacity, int* num_levels, int3
             if (samples) samples[i] = tree->level_samples[i];
             if (eval_ms) eval_ms[i] = tree->level_eval_ms[i];
         }
+    });
+}
+
+cf_status cf_tree_level_starts(cf_tree* tree, int capacity, float* start_ms) {
+    return guard([&] {
+        CF_REQUIRE(tree && start_ms, "cf_tree_level_starts: NULL argument");
+        const int m = std::min(static_cast<int>(tree->level_start_ms.size()), capacity);
+        for (int i = 0; i < m; i++) start_ms[i] = tree->level_start_ms[i];
     });
 }
 

@@ -23,6 +23,7 @@ struct cf_tree {
     std::vector<int32_t> level_nodes;     // open nodes evaluated per level
     std::vector<int64_t> level_samples;   // samples of those nodes
     std::vector<float> level_eval_ms;     // device time of the split search per level
+    std::vector<float> level_start_ms;    // start of each level's split search, ms after the tree's start
 
     void resize(int n) {
         num_nodes = n;

@@ -112,7 +112,7 @@ cf_status cf_context_device(cf_context* ctx, char* name, size_t name_length, int
  * write them back with set; set(NULL) restores the defaults. Results do not depend on the tuning,
  * only speed does. */
 typedef struct cf_eval_tuning {
-    int32_t features_per_tile;   /* features per shared-memory tile at most, 2..64 (default 32) */
+    int32_t features_per_tile;   /* features per shared-memory tile at most, 2..64 (default 16) */
     int32_t bins_budget_words;   /* histogram words per CTA, 1024..49152 (default 7168) */
     int32_t warp_aggregate;      /* 1: warp-aggregated shared increments, 0: plain atomics (default) */
     int32_t ctas_per_sm;         /* resident CTAs per SM the kernel is compiled for, 1..4 (default 3) */
@@ -355,6 +355,9 @@ cf_status cf_tree_train_stats(cf_tree* tree, int64_t* feature_evals, double* dev
  * (the reference logs per-level times, random_tree.h:1259,1411). Copies min(capacity, levels) entries. */
 cf_status cf_tree_level_stats(cf_tree* tree, int capacity, int* num_levels, int32_t* nodes, int64_t* samples,
                               float* eval_ms);
+/* Start of each level's split search in the last training, ms after the training's first device
+ * work (CUDA events; for lining per-level times up with clock and power samples). */
+cf_status cf_tree_level_starts(cf_tree* tree, int capacity, float* start_ms);
 
 /* ---------------------------------------------------------------------------------------------
  * Prediction: RandomForestImage::normalizeHistograms + convertTree + predict

@@ -819,6 +819,53 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
     return static_cast<int>(all.size());
 }
 
+/* Pixel-uniform sampling (random_tree_image.cpp:840-883): the image of each sample from one Sampler
+ * over the image list, its pixel from two fresh Samplers of the random source (x, then y), redrawn
+ * together while the label is ignored; then the block sort as above. Returns the count. */
+int orc_sample_pixel_uniform(int n, int width, int height, const uint8_t* labels, const uint16_t* depth_mm,
+                             const uint8_t* ignore, int subsample_count, int* seed_counter, int capacity,
+                             orc_sample* out) {
+    Sampler rgen_image = uniform_sampler(seed_counter, n);
+    const size_t hw = static_cast<size_t>(width) * height;
+    std::vector<orc_sample> all;
+    for (size_t k = 0; k < static_cast<size_t>(subsample_count) * n; k++) {
+        const int img = rgen_image.next();
+        Sampler rgen_x = uniform_sampler(seed_counter, width);
+        Sampler rgen_y = uniform_sampler(seed_counter, height);
+        for (long long tries = 0;; tries++) {
+            if (tries >= 100000000LL) return -1;
+            const int x = rgen_x.next(), y = rgen_y.next();
+            const size_t p = img * hw + static_cast<size_t>(y) * width + x;
+            if (ignore[labels[p]]) continue;
+            orc_sample s;
+            s.x = static_cast<uint16_t>(x);
+            s.y = static_cast<uint16_t>(y);
+            s.image = static_cast<uint32_t>(img);
+            const uint16_t d = depth_mm[p];
+            s.depth = d > 0 ? static_cast<float>(static_cast<int>(d)) / 1000.0f : 0.0f;
+            s.label = labels[p];
+            s.flip = 0;
+            s.reserved = 0;
+            all.push_back(s);
+            break;
+        }
+    }
+    const size_t block = 200000;
+    for (size_t b = 0; b < all.size(); b += block) {
+        const size_t e = std::min(all.size(), b + block);
+        std::stable_sort(all.begin() + b, all.begin() + e, [](const orc_sample& a, const orc_sample& c) {
+            if (a.image != c.image) return a.image < c.image;
+            if (a.label != c.label) return a.label < c.label;
+            if (a.y / 10 != c.y / 10) return a.y / 10 < c.y / 10;
+            if (a.x / 10 != c.x / 10) return a.x / 10 < c.x / 10;
+            return false;
+        });
+    }
+    if (static_cast<int>(all.size()) > capacity) return -2;
+    std::copy(all.begin(), all.end(), out);
+    return static_cast<int>(all.size());
+}
+
 /* RGBDImage::fillDepth (image.cpp:279-377): passes from the right, left, top and bottom, each
  * replacing a 0 by its already-processed neighbour. depth uint16 [n][H][W], in place. */
 void orc_fill_depth(int n, int width, int height, uint16_t* depth) {

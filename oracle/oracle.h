@@ -177,6 +177,10 @@ int orc_sample_class_uniform(int n, int width, int height, const uint8_t* labels
                              const uint16_t* depth_mm, int num_classes, const uint8_t* ignore,
                              int subsample_count, int* seed_counter, int capacity,
                              orc_sample* out);
+/* Pixel-uniform sampling (random_tree_image.cpp:840-883) with the block sort; returns the count. */
+int orc_sample_pixel_uniform(int n, int width, int height, const uint8_t* labels, const uint16_t* depth_mm,
+                             const uint8_t* ignore, int subsample_count, int* seed_counter, int capacity,
+                             orc_sample* out);
 /* RGBDImage::fillDepth (image.cpp:279-377) on depth uint16 [n][H][W], in place. */
 void orc_fill_depth(int n, int width, int height, uint16_t* depth);
 /* CIE 1976 L*a*b* (linear RGB / 255, BT.709 primaries, D65 white; the published formulas the

@@ -348,3 +348,19 @@ def synthetic_frames(seed, num_images, width, height, num_cells, num_classes, fi
     lib().orc_synthetic_frames(ctypes.c_uint64(seed), first, num_images, width, height, num_cells, num_classes,
                                _p(rgb), _p(depth), _p(labels))
     return rgb, depth, labels
+
+
+def sample_pixel_uniform(labels, depth_mm, ignore, subsample_count, seed_counter):
+    """Pixel-uniform sampling with the block sort; returns (count, samples, new seed counter)."""
+    labels = np.ascontiguousarray(labels, dtype=np.uint8)
+    depth_mm = np.ascontiguousarray(depth_mm, dtype=np.uint16)
+    ignore = np.ascontiguousarray(ignore, dtype=np.uint8)
+    n, h, w = labels.shape
+    cap = n * subsample_count
+    out = np.empty(cap, SAMPLE_DTYPE)
+    sc = ctypes.c_int(seed_counter)
+    rc = lib().orc_sample_pixel_uniform(n, w, h, _p(labels), _p(depth_mm), _p(ignore), subsample_count,
+                                        ctypes.byref(sc), cap, _p(out))
+    if rc < 0:
+        return rc, None, sc.value
+    return rc, out[:rc].copy(), sc.value

@@ -2,6 +2,7 @@
 // sample) evaluation is covered exactly once, chunk groups are consistent (same node and features,
 // contiguous sample slices in order, `chunks` members, at most one histogram tile of features), the
 // group limit holds, and the work order is a permutation. Prints one line per case, "ok" or "FAIL".
+#include <algorithm>
 #include <cstdio>
 #include <map>
 #include <vector>
@@ -54,6 +55,21 @@ static void check(const char* name, std::vector<int> counts, int F, int chunk_fe
     std::vector<int> seen(items.size(), 0);
     for (int o : order) seen[o]++;
     for (int s : seen) ok = ok && s == 1;
+    // chunked items first, chunk-major: (slice, group) never decreases along the order
+    bool in_chunked = true;
+    for (size_t q = 0; q < order.size(); q++) {
+        const EvalItem& it = items[order[q]];
+        if (it.chunks > 1) {
+            if (!in_chunked) ok = false;
+            if (q > 0) {
+                const EvalItem& pv = items[order[q - 1]];
+                if (pv.chunks > 1 && (pv.chunk > it.chunk || (pv.chunk == it.chunk && pv.group > it.group))) ok = false;
+            }
+            if (it.s_end - it.s_begin > std::max(kChunkTargetSamples, counts[it.node] / 2)) ok = false;
+        } else {
+            in_chunked = false;
+        }
+    }
     if (!ok) failures++;
     std::printf("%s: items %zu groups %d %s\n", name, items.size(), groups, ok ? "ok" : "FAIL");
 }

@@ -224,3 +224,18 @@ def test_reads_a_tree_file_laid_out_as_the_reference_writes_it(tmp_path):
     b = t2.arrays()
     for k in ("level", "left", "feature", "threshold", "feature_id", "histogram", "num_samples"):
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def test_pixel_uniform_sampling_matches_oracle():
+    """cf_sample_tree_pixels with pixelUniform (host form) vs the oracle's restatement of
+    random_tree_image.cpp:840-883 and the block sort."""
+    rgb, depth, labels = cf.synthetic_frames(4, 3, 64, 48, 10, 8)
+    cfg = cf.TrainConfig(samples_per_image=300, subsampling_type=1)
+    seed = cf.forest_seed(4711)
+    ignore = np.zeros(8, np.uint8)
+    ignore[0] = 1
+    s, prior, counter = cf.sample_tree_pixels(labels, depth, 8, cfg, 2, seed, ignored=ignore)
+    rc, o, ocounter = orc.sample_pixel_uniform(labels, depth, ignore, 150, seed)
+    assert rc == len(s) == 450 and counter == ocounter
+    np.testing.assert_array_equal(s.view(np.uint8), o.view(np.uint8))
+    assert (s["label"] != 0).all()

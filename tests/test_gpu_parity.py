@@ -407,6 +407,44 @@ def test_device_sampler_matches_oracle(ctx):
         cf.sample_tree_pixels(labels, depth, 6, train_cfg(samples_per_image=60000, sampler=1), 1, 77, ctx=ctx)
 
 
+def test_device_sampler_at_scale_matches_oracle(ctx):
+    """The device sampler's selection and ordering (radix sorts on the GPU) at 40 classes, 20 frames
+    640x480 and 8000 samples per frame, against the oracle's restatement."""
+    rgb, depth, labels = cf.synthetic_frames(2026, 20, 640, 480, 40, 40)
+    cfg = train_cfg(samples_per_image=80000, sampler=1)
+    s, prior, counter = cf.sample_tree_pixels(labels, depth, 40, cfg, 10, 4242, ctx=ctx)
+    rc, o, ocounter = orc.sample_class_uniform_keys(labels, depth, 40, np.zeros(40, np.uint8), 8000, 4242)
+    assert rc == len(s) == 40 * 4000 and counter == ocounter
+    for k in ("x", "y", "image", "label", "flip"):
+        np.testing.assert_array_equal(s[k], o[k], err_msg=k)
+    np.testing.assert_array_equal(s["depth"].view(np.uint32), o["depth"].view(np.uint32))
+    np.testing.assert_array_equal(prior, np.bincount(labels.ravel(), minlength=40))
+
+
+@pytest.mark.parametrize("shape", [(3, 64, 48, 8, 300), (4, 640, 480, 40, 8000)])
+def test_device_pixel_uniform_sampler_matches_oracle(ctx, shape):
+    """pixelUniform on the device (the reference's random streams, one thread per sample) against the
+    oracle's restatement of random_tree_image.cpp:840-883 with the block sort, void class ignored."""
+    n, w, h, C, per_image = shape
+    rgb, depth, labels = cf.synthetic_frames(4, n, w, h, 10, C)
+    ign = np.zeros(C, np.uint8)
+    ign[0] = 1
+    cfg = train_cfg(samples_per_image=2 * per_image, subsampling_type=1, sampler=1)
+    seed = cf.forest_seed(4711)
+    s, prior, counter = cf.sample_tree_pixels(labels, depth, C, cfg, 2, seed + 1, ignored=ign, ctx=ctx)
+    rc, o, ocounter = orc.sample_pixel_uniform(labels, depth, ign, per_image, seed + 1)
+    assert rc == len(s) == n * per_image and counter == ocounter
+    for k in ("x", "y", "image", "label", "flip"):
+        np.testing.assert_array_equal(s[k], o[k], err_msg=k)
+    np.testing.assert_array_equal(s["depth"].view(np.uint32), o["depth"].view(np.uint32))
+    np.testing.assert_array_equal(prior, np.bincount(labels.ravel(), minlength=C))
+    assert (s["label"] != 0).all()
+    # the host form of the same definition gives the same samples
+    hs, _, hcounter = cf.sample_tree_pixels(labels, depth, C, cfg, 2, seed + 1, ignored=ign)
+    assert hcounter == counter
+    np.testing.assert_array_equal(hs.view(np.uint8), s.view(np.uint8))
+
+
 def test_forest_train_device_sampler_matches_oracle(ctx):
     rgb, depth, labels = H.frames(seed=6, n=3, w=80, h=60, cells=10, classes=6)
     cfg = train_cfg(random_seed=4711, samples_per_image=120, max_depth=7, sampler=1)

@@ -42,7 +42,7 @@ def scene(ctx):
 def test_default_tuning_and_reset(ctx):
     ctx.set_tuning()
     d = ctx.get_tuning().as_dict()
-    assert d["ctas_per_sm"] == 3 and d["warp_aggregate"] == 0 and d["features_per_tile"] == 32
+    assert d["ctas_per_sm"] == 3 and d["warp_aggregate"] == 0 and d["features_per_tile"] == 16
     assert d["sample_groups"] == 1
     ctx.set_tuning(items_per_slot=2.0)
     assert ctx.get_tuning().items_per_slot == 2.0
