@@ -887,6 +887,8 @@ def main():
     ap.add_argument("--no-per-node", action="store_true", help="skip the plain per-node comparisons")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default split-search launch shape")
     ap.add_argument("--headline-only", action="store_true", help="skip configs 1, 2, 4 and 5")
+    ap.add_argument("--sections", default="headline,config1,config2,predict",
+                    help="comma-separated parts to run (profiling runs pick one); predict needs config2's forest data")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="Poisson load per offered rate (0: skip)")
     ap.add_argument("--tuning", default="", help="split-search launch shape overrides, e.g. ctas_per_sm=4,"
                     "bins_budget_words=10240 (cf_eval_tuning field names)")
@@ -936,20 +938,35 @@ def main():
     ctx.set_stream(stream.cuda_stream)
 
     C3["images"] = args.images
+    sections = set(args.sections.split(","))
+    if "headline" not in sections:
+        # a profiling run of other parts only
+        if "config1" in sections:
+            config1(ctx, stream)
+        if "config2" in sections or "predict" in sections:
+            c2, ds2, (rgb2, depth2, labels2) = config2(ctx, stream, args)
+            if "predict" in sections:
+                ptrees = forest_trees(ds2, rgb2, depth2, labels2, C4["trees"])
+                predict_section(ctx, stream, ds2, ptrees, local, args.serve_seconds)
+        ctx.close()
+        return
     head = headline(ctx, stream, local, rank, world, args, barrier, max_over_ranks, sum_over_ranks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_train()
     extra = {}
     if rank == 0 and world == 1 and not args.headline_only:
-        extra["config1"] = config1(ctx, stream)
-        c2, ds2, (rgb2, depth2, labels2) = config2(ctx, stream, args)
-        extra["config2"] = c2
-        ptrees = forest_trees(ds2, rgb2, depth2, labels2, C4["trees"])
-        extra["predict"] = predict_section(ctx, stream, ds2, ptrees, local, args.serve_seconds)
-        for t in ptrees:
-            t.close()
-        ds2.close()
+        if "config1" in sections:
+            extra["config1"] = config1(ctx, stream)
+        if "config2" in sections or "predict" in sections:
+            c2, ds2, (rgb2, depth2, labels2) = config2(ctx, stream, args)
+            extra["config2"] = c2
+            if "predict" in sections:
+                ptrees = forest_trees(ds2, rgb2, depth2, labels2, C4["trees"])
+                extra["predict"] = predict_section(ctx, stream, ds2, ptrees, local, args.serve_seconds)
+                for t in ptrees:
+                    t.close()
+            ds2.close()
     if rank == 0:
         line = {"metric": METRIC, "value": head["value"], "unit": "feature-evals/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
