@@ -132,14 +132,14 @@ __device__ __forceinline__ EvalFeat make_eval_feat(const FeatParams& f) {
     return e;
 }
 
-// Thresholds of one feature in shared memory: sorted ascending. With kPad = 32 (T <= 32) or 64
-// (33 <= T <= 63) the row has kPad entries, positions T..kPad-1 holding +inf, and is searched
-// branch-free in five or six steps (a full row of 32 yields counts 0..32); kPad = 0 keeps the T
-// thresholds and a binary search.
+// Thresholds of one feature in shared memory: sorted ascending. With kPad = 32 (T <= 31) or 64
+// (32 <= T <= 63) the row has kPad entries, positions T..kPad-1 holding +inf, and is searched
+// branch-free in five or six steps; kPad = 0 keeps the T thresholds and a binary search. (Five steps
+// give 32 outcomes, counts 0..31, so a row of 32 serves T <= 31 only.)
 constexpr int kPadThresholds = 32;
 
 // the padded row width for T thresholds (0: no padding)
-__host__ __device__ constexpr int padded_row(int T) { return T <= 32 ? 32 : (T < 64 ? 64 : 0); }
+__host__ __device__ constexpr int padded_row(int T) { return T < 32 ? 32 : (T < 64 ? 64 : 0); }
 
 // #{i : sorted[i] < v}
 template <int kPad>

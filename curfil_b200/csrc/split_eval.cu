@@ -733,7 +733,7 @@ void launch_level_eval_a(cf_context* ctx, const EvalArgs& args, int grid, size_t
     }
 }
 
-// The level_eval instance for the tuning and threshold count (T <= 32 and 33 <= T <= 63 take the
+// The level_eval instance for the tuning and threshold count (T <= 31 and 32 <= T <= 63 take the
 // padded branch-free searches).
 void launch_level_eval(cf_context* ctx, const EvalArgs& args, int grid, const EvalTuning& tuning) {
     int budget = 0;
