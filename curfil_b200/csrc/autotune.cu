@@ -86,8 +86,9 @@ extern "C" cf_status cf_autotune_split_search(cf_dataset* ds, int num_samples, c
         double cur_ms = measure(cur);
         if (start_ms) *start_ms = cur_ms;
         const int budgets[] = {4096, 6144, 7168, 8192, 10240, 12288};
-        const float slots[] = {16.0f, 32.0f, 64.0f, 128.0f};
+        const float slots[] = {64.0f, 256.0f, 1024.0f, 2048.0f, 4096.0f};
         const int granules[] = {4, 8, 16};
+        const int min_evals[] = {4096, 16384, 65536};
         const int tiles[] = {16, 32};
         for (int pass = 0; pass < 2; pass++) {
             bool improved = false;
@@ -120,6 +121,16 @@ extern "C" cf_status cf_autotune_split_search(cf_dataset* ds, int num_samples, c
             for (int v : granules) {
                 cf_eval_tuning c = cur;
                 c.feature_granule = v;
+                consider(c);
+            }
+            for (int v : min_evals) {
+                cf_eval_tuning c = cur;
+                c.min_item_evals = v;
+                consider(c);
+            }
+            for (int v = 0; v <= 1; v++) {
+                cf_eval_tuning c = cur;
+                c.stage_bins = v;
                 consider(c);
             }
             for (int v : tiles) {

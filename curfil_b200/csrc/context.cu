@@ -108,6 +108,7 @@ cf_status cf_context_create(int device, cf_context** out) {
         ctx->device = device;
         ctx->num_sms = prop.multiProcessorCount;
         ctx->smem_per_block_optin = prop.sharedMemPerBlockOptin;
+        ctx->l2_bytes = static_cast<size_t>(prop.l2CacheSize);
         cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) {
             delete ctx;
@@ -224,9 +225,14 @@ cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning) {
         CF_REQUIRE(t.ctas_per_sm >= 1 && t.ctas_per_sm <= 4, "cf_context_set_tuning: ctas_per_sm must be in [1, 4]");
         CF_REQUIRE(t.feature_granule >= 1 && t.feature_granule <= 64,
                    "cf_context_set_tuning: feature_granule must be in [1, 64]");
-        CF_REQUIRE(t.items_per_slot > 0.0f && t.items_per_slot <= 1024.0f,
-                   "cf_context_set_tuning: items_per_slot must be in (0, 1024]");
+        CF_REQUIRE(t.items_per_slot > 0.0f && t.items_per_slot <= 8192.0f,
+                   "cf_context_set_tuning: items_per_slot must be in (0, 8192]");
         CF_REQUIRE(t.sample_groups == 0 || t.sample_groups == 1, "cf_context_set_tuning: sample_groups is 0 or 1");
+        CF_REQUIRE(t.min_item_evals >= 256 && t.min_item_evals <= (1 << 30),
+                   "cf_context_set_tuning: min_item_evals must be in [256, 2^30]");
+        CF_REQUIRE(t.stage_bins >= 0 && t.stage_bins <= 2, "cf_context_set_tuning: stage_bins must be 0, 1 or 2");
+        CF_REQUIRE(t.stage_max_mb >= 1 && t.stage_max_mb <= 65536,
+                   "cf_context_set_tuning: stage_max_mb must be in [1, 65536]");
         std::lock_guard<std::mutex> lock(ctx->mu);
         ctx->tuning = t;
     });

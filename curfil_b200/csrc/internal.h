@@ -135,6 +135,7 @@ struct cf_context {
     int device = 0;
     int num_sms = 0;
     size_t smem_per_block_optin = 0;
+    size_t l2_bytes = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     bool timing = false;
@@ -149,12 +150,13 @@ struct cf_context {
     void (*spare_trainer_free)(void*) = nullptr;
 
     // measured on B200 with 200 frames 640x480, 40 classes, 2000 features x 20 thresholds: a 28 KB
-    // histogram leaves ~140 KB of the SM's unified memory to L1 for the integral-image gathers, and
-    // ~64 items per CTA slot keep the last wave of a level short; sample groups without increment
-    // aggregation were 8 % faster than thread-per-sample with aggregation. With 1000 frames and
-    // 4000 features x 32 thresholds, tiles of at most 16 features (shared staging sized for 16, not
-    // 32) left more L1 and were 3-12 % faster per level.
-    static cf_eval_tuning default_tuning() { return cf_eval_tuning{16, 7168, 0, 3, 8, 64.0f, 1}; }
+    // histogram leaves ~140 KB of the SM's unified memory to L1 for the integral-image gathers; sample
+    // groups without increment aggregation were 8 % faster than thread-per-sample with aggregation.
+    // With 1000 frames and 4000 features x 32 thresholds, tiles of at most 16 features (shared staging
+    // sized for 16, not 32) left more L1 and were 3-12 % faster per level. Up to 2048 items per CTA
+    // slot of at least 16 K evaluations, in multiples of 4 features, were 4-21 % faster on the levels
+    // of that workload (more CTAs on one node's samples at a time, sharing their gathers in L2).
+    static cf_eval_tuning default_tuning() { return cf_eval_tuning{16, 7168, 0, 3, 4, 2048.0f, 1, 16384, 1, 8192}; }
     std::mutex mu;
     struct KernelEvents {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;

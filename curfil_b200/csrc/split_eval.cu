@@ -23,6 +23,8 @@
 #include <cstring>
 #include <limits>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "eval_fast.cuh"
 #include "split_eval.h"
 
@@ -32,6 +34,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kUnroll = 2;   // samples per lane and step in the sample-group mapping (4 spills and is slower)
+constexpr int kStagedUnroll = 2;   // samples per lane and step in the staged-bins histogram (4 was no faster)
 
 template <bool kAgg>
 __device__ __forceinline__ void bin_increment(uint32_t* bins, int key) {
@@ -42,6 +45,33 @@ __device__ __forceinline__ void bin_increment(uint32_t* bins, int key) {
     } else {
         if (key >= 0) atomicAdd(bins + key, 1u);
     }
+}
+
+// Scoring constants of one node: the sample total, the classification entropy and the constants of
+// the score bounds, all over the present classes in ascending label order.
+struct NodeConsts {
+    double total, hc;
+    ScoreConsts k;
+};
+
+// One thread per node: the constants every work item of the node would otherwise compute on one
+// thread (a few double logarithms per class) while the CTA waits.
+__global__ void node_consts_kernel(int M, int C, const uint32_t* __restrict__ node_hist, NodeConsts* __restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M) return;
+    uint32_t counts[256];
+    int cp = 0;
+    for (int c = 0; c < C; c++) {
+        const uint32_t h = node_hist[static_cast<long long>(n) * C + c];
+        if (h > 0) counts[cp++] = h;
+    }
+    double total = 0;
+    for (int i = 0; i < cp; i++) total += static_cast<double>(counts[i]);
+    NodeConsts r;
+    r.total = total;
+    r.hc = classification_entropy(cp, counts, total);
+    r.k = score_consts(counts, cp);
+    out[n] = r;
 }
 
 struct EvalArgs {
@@ -63,6 +93,15 @@ struct EvalArgs {
     uint32_t* group_bins;  // [groups][bins_budget] merged counts of chunked items, zero at launch
     int* group_count;      // [groups] chunks finished, zero at launch
     uint32_t* dump_left;   // optional [M][F][T][C] left counts (tests); nullptr in training
+    // staged bins: the bin of row r, feature f is staged[r * staged_stride + f - staged_f0]; the rows of
+    // node n start at row_base[n]. nullptr: the kernel computes its bins itself.
+    const uint8_t* staged = nullptr;
+    long long staged_stride = 0;
+    int staged_f0 = 0;
+    const long long* row_base = nullptr;
+    // per-node scoring constants computed once per level (node_consts_kernel); nullptr: every item
+    // computes its node's constants itself
+    const NodeConsts* node_consts = nullptr;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -144,6 +183,8 @@ level_eval_kernel(EvalArgs a) {
     __shared__ double s_best;
     __shared__ double s_cs[kMaxCand];
     __shared__ int s_ct[kMaxCand], s_cf[kMaxCand];
+    __shared__ double s_ns[kMaxCand];   // a tile's new candidates
+    __shared__ int s_nt[kMaxCand], s_nf[kMaxCand];
     __shared__ int s_cn;
     __shared__ double s_drop;
     __shared__ int s_last;
@@ -197,17 +238,25 @@ level_eval_kernel(EvalArgs a) {
                 s_best = -INFINITY;
                 s_cn = 0;
                 s_drop = -INFINITY;
+                if (a.node_consts) {
+                    const NodeConsts nc = a.node_consts[item.node];
+                    s_total = nc.total;
+                    s_hc = nc.hc;
+                    s_k = nc.k;
+                }
             }
             __syncthreads();
-            if (tid == 0) {
-                // node total and classification entropy, classes in ascending label order (score.h:174-189)
-                double total = 0;
-                for (int i = 0; i < s_cp; i++) total += static_cast<double>(s_counts[i]);
-                s_total = total;
-                s_hc = classification_entropy(s_cp, s_counts, total);
-                s_k = score_consts(s_counts, s_cp);
+            if (!a.node_consts) {
+                if (tid == 0) {
+                    // node total and classification entropy, classes in ascending label order (score.h:174-189)
+                    double total = 0;
+                    for (int i = 0; i < s_cp; i++) total += static_cast<double>(s_counts[i]);
+                    s_total = total;
+                    s_hc = classification_entropy(s_cp, s_counts, total);
+                    s_k = score_consts(s_counts, s_cp);
+                }
+                __syncthreads();
             }
-            __syncthreads();
         }
         const ScoreConsts sk = s_k;
         const int cp = s_cp;
@@ -240,8 +289,69 @@ level_eval_kernel(EvalArgs a) {
 
             const int W = a.ds.width, H = a.ds.height;
             const int nthr = blockDim.x;
-            const int n_major = kGrouped ? 0 : (N / nthr) * nthr;
-            if constexpr (kGrouped) {
+            const int n_major = kGrouped || a.staged ? 0 : (N / nthr) * nthr;
+            if (a.staged) {
+                // ---- histogram of staged bins: the tile's bins of one sample are nw 4-byte words of its
+                // row (the segment starts `lead` bytes into the first); WL lanes (nw rounded up to a
+                // power of two) take one sample, a lane one word, i.e. four bins, and each lane
+                // kStagedUnroll samples per step so that many loads are in flight. A sample evaluated
+                // both ways (flip 2) has its unflipped bin staged; the flipped one is computed here by
+                // the sample's first lane.
+                const long long off = f0 - a.staged_f0;
+                const int lead = static_cast<int>(off & 3);
+                const int nw = (lead + nf + 3) >> 2;
+                const int WL = nw <= 1 ? 1 : 1 << (32 - __clz(nw - 1));
+                const int wi = lane & (WL - 1);
+                const int js = lane / WL;
+                const int step = static_cast<int>(blockDim.x >> 5) * (32 / WL);
+                const uint8_t* rows =
+                    a.staged + (a.row_base[item.node] + (sbase - nd.start)) * a.staged_stride + (off - lead);
+                for (int s0 = warp * (32 / WL); s0 < N; s0 += kStagedUnroll * step) {   // trip count uniform in a warp
+                    uint32_t v[kStagedUnroll];
+                    int lid[kStagedUnroll], flip[kStagedUnroll];
+                    bool act[kStagedUnroll];
+                    Sample smp[kStagedUnroll];
+#pragma unroll
+                    for (int u = 0; u < kStagedUnroll; u++) {
+                        const int s = s0 + js + u * step;
+                        const bool sv = s < N;
+                        const int sc = sv ? s : N - 1;
+                        smp[u] = a.samples[sbase + sc];
+                        act[u] = sv && wi < nw;
+                        v[u] = act[u] ? __ldg(reinterpret_cast<const uint32_t*>(rows + static_cast<long long>(sc) *
+                                                                                            a.staged_stride) + wi)
+                                      : 0u;
+                        flip[u] = sv && wi == 0 ? smp[u].flip : 0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kStagedUnroll; u++) {
+                        lid[u] = s_lid[smp[u].label];
+#pragma unroll
+                        for (int b = 0; b < 4; b++) {
+                            const int f = 4 * wi + b - lead;
+                            const bool ok = act[u] && f >= 0 && f < nf;
+                            bin_increment<kAgg>(s_bins,
+                                                ok ? (f * cp + lid[u]) * T1 + static_cast<int>((v[u] >> (8 * b)) & 0xffu) : -1);
+                        }
+                    }
+                    bool both = false;
+#pragma unroll
+                    for (int u = 0; u < kStagedUnroll; u++) both = both || flip[u] == 2;
+                    if (__any_sync(kFull, both)) {
+#pragma unroll
+                        for (int u = 0; u < kStagedUnroll; u++) {
+                            const EvalPixel px = make_eval_pixel(a.ds, smp[u]);
+                            for (int f = 0; f < nf; f++) {
+                                const SortedBins<kPad> sorted{s_thr + f * TPS, T};
+                                const int key = flip[u] == 2
+                                                    ? (f * cp + lid[u]) * T1 + feature_bin(px, W, H, s_params[f], true, sorted)
+                                                    : -1;
+                                bin_increment<kAgg>(s_bins, key);
+                            }
+                        }
+                    }
+                }
+            } else if constexpr (kGrouped) {
                 // ---- histogram, sample groups: the lanes of a warp take (sample, feature) pairs of a
                 // few consecutive samples (FL lanes per sample, FL = nf rounded up to a power of two,
                 // at most 32) and the warps of the CTA the next groups. The samples in flight on an SM
@@ -357,7 +467,7 @@ level_eval_kernel(EvalArgs a) {
             }
             // ---- the remaining Nt < blockDim samples, pair-major: pairs p = f * Nt + s spread over
             // all threads with a uniform trip count so warps stay converged
-            const int Nt = N - n_major;
+            const int Nt = a.staged ? 0 : N - n_major;
             if (!kGrouped && Nt > 0) {
                 const Sample* tail = a.samples + sbase + n_major;
                 const long long pairs = static_cast<long long>(nf) * Nt;
@@ -409,13 +519,32 @@ level_eval_kernel(EvalArgs a) {
                 __syncthreads();
             }
 
-            // ---- cumulative counts along the threshold positions
-            for (int row = tid; row < nf * cp; row += blockDim.x) {
-                uint32_t acc = 0;
-                uint32_t* b = s_bins + row * T1;
-                for (int k = 0; k < T1; k++) {
-                    acc += b[k];
-                    b[k] = acc;
+            // ---- cumulative counts along the threshold positions: a thread per row, or where the
+            // tile has few rows (few classes present) a warp per row, 32 positions per shuffle scan
+            if (nf * cp > 128) {
+                for (int row = tid; row < nf * cp; row += blockDim.x) {
+                    uint32_t acc = 0;
+                    uint32_t* b = s_bins + row * T1;
+                    for (int k = 0; k < T1; k++) {
+                        acc += b[k];
+                        b[k] = acc;
+                    }
+                }
+            } else {
+                for (int row = warp; row < nf * cp; row += static_cast<int>(blockDim.x >> 5)) {
+                    uint32_t* b = s_bins + row * T1;
+                    uint32_t carry = 0;
+                    for (int k0 = 0; k0 < T1; k0 += 32) {
+                        const int k = k0 + lane;
+                        uint32_t v = k < T1 ? b[k] : 0u;
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const uint32_t u = __shfl_up_sync(kFull, v, o);
+                            if (lane >= o) v += u;
+                        }
+                        v += carry;
+                        if (k < T1) b[k] = v;
+                        carry = __shfl_sync(kFull, v, 31);
+                    }
                 }
             }
             __syncthreads();
@@ -488,40 +617,56 @@ level_eval_kernel(EvalArgs a) {
                     s_best = mnew;
                 }
                 __syncwarp();
+                // the tile's pairs inside the window in key order (threshold, then feature), all lanes
+                // at once: the first kMaxCand are merged into the list, the others only raise the
+                // dropped score (a tile of tied scores is kMaxCand insertions, not n)
+                int taken = 0;
+                double dmax = -INFINITY;
                 for (int base = 0; base < n; base += 32) {
-                    const int i = base + lane;
-                    const bool e = i < n && __dsub_rn(mnew, s_scores[i]) < 1e-13;
-                    unsigned bal = __ballot_sync(kFull, e);
-                    if (lane == 0) {
-                        while (bal) {
-                            const int b = __ffs(bal) - 1;
-                            bal &= bal - 1;
-                            const int ii = base + b;
-                            const int fl = ii / T;
-                            const int t = ii - fl * T;
-                            const int fg = f0 + fl;
-                            const long long key = static_cast<long long>(t) * a.F + fg;
-                            int pos = s_cn;
-                            while (pos > 0 && static_cast<long long>(s_ct[pos - 1]) * a.F + s_cf[pos - 1] > key) pos--;
-                            if (pos >= kMaxCand) {
-                                s_drop = fmax(s_drop, s_scores[ii]);
-                                continue;
-                            }
-                            if (s_cn == kMaxCand) s_drop = fmax(s_drop, s_cs[kMaxCand - 1]);
-                            const int last = min(s_cn, kMaxCand - 1);
-                            for (int j = last; j > pos; j--) {
-                                s_cs[j] = s_cs[j - 1];
-                                s_ct[j] = s_ct[j - 1];
-                                s_cf[j] = s_cf[j - 1];
-                            }
-                            s_cs[pos] = s_scores[ii];
-                            s_ct[pos] = t;
-                            s_cf[pos] = fg;
-                            s_cn = min(s_cn + 1, kMaxCand);
-                        }
+                    const int p = base + lane;
+                    const int t = p / nf;
+                    const int fl = p - t * nf;
+                    const double sc = p < n ? s_scores[fl * T + t] : -INFINITY;
+                    const bool e = p < n && __dsub_rn(mnew, sc) < 1e-13;
+                    const unsigned bal = __ballot_sync(kFull, e);
+                    const int rank = taken + __popc(bal & ((1u << lane) - 1u));
+                    if (e && rank < kMaxCand) {
+                        s_ns[rank] = sc;
+                        s_nt[rank] = t;
+                        s_nf[rank] = f0 + fl;
+                    } else if (e) {
+                        dmax = fmax(dmax, sc);
                     }
-                    __syncwarp();
+                    taken = min(kMaxCand, taken + __popc(bal));
                 }
+                for (int off = 16; off > 0; off >>= 1) dmax = fmax(dmax, __shfl_xor_sync(kFull, dmax, off));
+                __syncwarp();
+                if (lane == 0) {
+                    s_drop = fmax(s_drop, dmax);
+                    for (int q = 0; q < taken; q++) {
+                        const int t = s_nt[q];
+                        const int fg = s_nf[q];
+                        const long long key = static_cast<long long>(t) * a.F + fg;
+                        int pos = s_cn;
+                        while (pos > 0 && static_cast<long long>(s_ct[pos - 1]) * a.F + s_cf[pos - 1] > key) pos--;
+                        if (pos >= kMaxCand) {
+                            s_drop = fmax(s_drop, s_ns[q]);
+                            continue;
+                        }
+                        if (s_cn == kMaxCand) s_drop = fmax(s_drop, s_cs[kMaxCand - 1]);
+                        const int last = min(s_cn, kMaxCand - 1);
+                        for (int j = last; j > pos; j--) {
+                            s_cs[j] = s_cs[j - 1];
+                            s_ct[j] = s_ct[j - 1];
+                            s_cf[j] = s_cf[j - 1];
+                        }
+                        s_cs[pos] = s_ns[q];
+                        s_ct[pos] = t;
+                        s_cf[pos] = fg;
+                        s_cn = min(s_cn + 1, kMaxCand);
+                    }
+                }
+                __syncwarp();
             }
             __syncthreads();
         }
@@ -542,34 +687,141 @@ level_eval_kernel(EvalArgs a) {
     }
 }
 
-// One thread per node: global tie rule over the candidates of the node's items.
+// ---- staged bins, pass 1 -------------------------------------------------------------------------
+// Rows of the staged table: row_base[n] + k is sample k of node n. stage_rows_kernel gives every row
+// its sample's position in the level's array and its pixel (frame, y, x) as the sort key of the pass-1
+// order: frame by frame, and within a frame in raster order, so neighbouring threads take samples
+// whose neighbourhoods overlap.
+__global__ void stage_rows_kernel(const NodeDesc* __restrict__ nodes, const long long* __restrict__ row_base, int M,
+                                  long long rows, const Sample* __restrict__ samples, int W, long long plane,
+                                  int* __restrict__ row_pos, unsigned long long* __restrict__ pixel_key,
+                                  int* __restrict__ row_ids) {
+    const long long r = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (r >= rows) return;
+    int lo = 0, hi = M - 1;   // the last node n with row_base[n] <= r
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (row_base[mid] <= r) lo = mid;
+        else hi = mid - 1;
+    }
+    const long long p = nodes[lo].start + (r - row_base[lo]);
+    const Sample s = samples[p];
+    row_pos[r] = static_cast<int>(p);
+    pixel_key[r] = static_cast<unsigned long long>(s.image) * plane + static_cast<long long>(s.y) * W + s.x;
+    row_ids[r] = static_cast<int>(r);
+}
+
+struct StageArgs {
+    DsView ds;
+    const Sample* samples;
+    const int* frame_order;   // [rows] rows sorted by frame (stable)
+    const int* row_pos;       // [rows] sample position of each row
+    long long rows;
+    const FeatParams* packs;
+    const float* sorted_thr;  // [F][T]
+    int T;
+    int f_first, n_feat;      // this chunk's features [f_first, f_first + n_feat)
+    long long stride;         // row bytes, a multiple of kStageTile
+    uint8_t* out;
+};
+
+// One work item = 256 consecutive rows of the frame order x one tile of kStageTile features; items are
+// taken row-block-major, so the resident CTAs evaluate the samples of one or two frames at a time and
+// their corner gathers hit L2. A thread takes one sample through the tile's features (two at a time,
+// their gathers overlapping) and stores each four bins as one word of its row. The bin is that of the
+// fused kernel's feature_bin: the unflipped response for flip 0 and 2, the flipped one for flip 1.
+constexpr int kStageCtasPerSm = 3;   // 4 (56 registers fit) was 5-7 % slower: less L1 per CTA
+
+template <int kPad>
+__global__ void __launch_bounds__(256, kStageCtasPerSm)
+stage_bins_kernel(StageArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    EvalFeat* s_params = reinterpret_cast<EvalFeat*>(smem);
+    float* s_thr = reinterpret_cast<float*>(smem + sizeof(EvalFeat) * kStageTile);
+    const int T = a.T;
+    const int TP = kPad ? kPad : T;
+    const int W = a.ds.width, H = a.ds.height;
+    const int tiles = (a.n_feat + kStageTile - 1) / kStageTile;
+    const long long blocks = (a.rows + 255) / 256;
+    const long long n_items = blocks * tiles;
+    for (long long q = blockIdx.x; q < n_items; q += gridDim.x) {
+        const long long blk = q / tiles;
+        const int j = static_cast<int>(q - blk * tiles);
+        const int fb = j * kStageTile;
+        const int nf = min(kStageTile, a.n_feat - fb);
+        const int fg = a.f_first + fb;
+        __syncthreads();   // the previous item's reads of the tile are done
+        for (int i = threadIdx.x; i < nf; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[fg + i]);
+        const float* g_thr = a.sorted_thr + static_cast<long long>(fg) * T;
+        for (int i = threadIdx.x; i < nf * TP; i += blockDim.x) {
+            const int f = i / TP, t = i - f * TP;
+            s_thr[i] = t < T ? g_thr[f * T + t] : INFINITY;
+        }
+        __syncthreads();
+        const long long r = blk * 256 + threadIdx.x;
+        if (r < a.rows) {
+            const int row = a.frame_order[r];
+            const Sample smp = a.samples[a.row_pos[row]];
+            const EvalPixel px = make_eval_pixel(a.ds, smp);
+            const bool flip = smp.flip == 1;
+            uint32_t* dst = reinterpret_cast<uint32_t*>(a.out + static_cast<long long>(row) * a.stride + fb);
+            uint32_t acc = 0;
+            for (int f = 0; f < nf; f += 2) {
+                const int b0 = feature_bin(px, W, H, s_params[f], flip, SortedBins<kPad>{s_thr + f * TP, T});
+                const int b1 =
+                    f + 1 < nf ? feature_bin(px, W, H, s_params[f + 1], flip, SortedBins<kPad>{s_thr + (f + 1) * TP, T}) : 0;
+                acc |= static_cast<uint32_t>(b0 | (b1 << 8)) << (8 * (f & 3));
+                if ((f & 3) == 2 || f + 2 >= nf) {
+                    dst[f >> 2] = acc;
+                    acc = 0;
+                }
+            }
+        }
+    }
+}
+
+// One warp per node: the global tie rule over the candidates of the node's items. The lanes stride
+// over the items; the best score is a max-reduction and the chosen candidate the lowest (threshold,
+// feature) key within the 1e-13 window, a min-reduction, so the result does not depend on how the
+// items are spread over the lanes. (The top levels' sliced nodes have up to ~10^5 items.)
 __global__ void reduce_candidates_kernel(int M, int F, const int* __restrict__ item_range,
                                          const ItemCandidates* __restrict__ cands, const float* __restrict__ thr,
                                          cf_split* __restrict__ out) {
-    const int node = blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= M) return;
+    const int lane = threadIdx.x & 31;
+    const int node = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
+    if (node >= M) return;   // uniform per warp
     const int b = item_range[node], e = item_range[node + 1];
     double m = -INFINITY;
-    for (int i = b; i < e; i++) m = fmax(m, cands[i].best);
+    for (int i = b + lane; i < e; i += 32) m = fmax(m, cands[i].best);
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(kFull, m, off));
     int ovf = 0;
-    for (int i = b; i < e; i++) ovf |= __dsub_rn(m, cands[i].dropped) < 1e-13 ? 1 : 0;
     long long best_key = LLONG_MAX;
     double best_s = m;
-    int bt = 0, bf = 0;
-    for (int i = b; i < e; i++) {
+    for (int i = b + lane; i < e; i += 32) {
         const ItemCandidates& c = cands[i];
+        ovf |= __dsub_rn(m, c.dropped) < 1e-13 ? 1 : 0;
         for (int j = 0; j < c.n; j++) {
             if (__dsub_rn(m, c.s[j]) < 1e-13) {
                 const long long key = static_cast<long long>(c.t[j]) * F + c.f[j];
                 if (key < best_key) {
                     best_key = key;
                     best_s = c.s[j];
-                    bt = c.t[j];
-                    bf = c.f[j];
                 }
             }
         }
     }
+    ovf = __any_sync(kFull, ovf) ? 1 : 0;
+    for (int off = 16; off > 0; off >>= 1) {
+        const long long k2 = __shfl_xor_sync(kFull, best_key, off);
+        const double s2 = __shfl_xor_sync(kFull, best_s, off);
+        if (k2 < best_key) {
+            best_key = k2;
+            best_s = s2;
+        }
+    }
+    if (lane != 0) return;
+    const int bt = best_key == LLONG_MAX ? 0 : static_cast<int>(best_key / F);
+    const int bf = best_key == LLONG_MAX ? 0 : static_cast<int>(best_key - static_cast<long long>(bt) * F);
     cf_split r;
     r.score = best_s;
     r.feature = bf;
@@ -733,6 +985,24 @@ void launch_level_eval_a(cf_context* ctx, const EvalArgs& args, int grid, size_t
     }
 }
 
+template <int kPad>
+void launch_stage_bins_t(cf_context* ctx, const StageArgs& a) {
+    const int TP = kPad ? kPad : a.T;
+    const size_t smem = sizeof(EvalFeat) * kStageTile + sizeof(float) * kStageTile * TP;
+    set_level_eval_smem(stage_bins_kernel<kPad>, smem, kStageCtasPerSm);
+    const long long items = (a.rows + 255) / 256 * ((a.n_feat + kStageTile - 1) / kStageTile);
+    const int grid = static_cast<int>(std::min<long long>(items, static_cast<long long>(ctx->num_sms) * kStageCtasPerSm));
+    launch(ctx, "stage_bins", dim3(grid), dim3(256), smem, stage_bins_kernel<kPad>, a);
+}
+
+void launch_stage_bins(cf_context* ctx, const StageArgs& a) {
+    switch (padded_row(a.T)) {
+        case 32: launch_stage_bins_t<32>(ctx, a); break;
+        case 64: launch_stage_bins_t<64>(ctx, a); break;
+        default: launch_stage_bins_t<0>(ctx, a); break;
+    }
+}
+
 // The level_eval instance for the tuning and threshold count (T <= 31 and 32 <= T <= 63 take the
 // padded branch-free searches).
 void launch_level_eval(cf_context* ctx, const EvalArgs& args, int grid, const EvalTuning& tuning) {
@@ -762,6 +1032,9 @@ EvalTuning EvalTuning::of(cf_context* ctx) {
     e.items_per_slot = t.items_per_slot;
     e.feature_granule = t.feature_granule;
     e.sample_groups = t.sample_groups;
+    e.min_item_evals = t.min_item_evals;
+    e.stage_bins = t.stage_bins;
+    e.stage_max_mb = t.stage_max_mb;
     return e;
 }
 
@@ -772,7 +1045,10 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
     const int g = std::max(1, tuning.feature_granule);
     long long total_work = 0;
     for (int n : node_counts) total_work += static_cast<long long>(n) * F;
-    const double target_items = tuning.items_per_slot * slots;
+    // items_per_slot items per resident CTA, or fewer where that would make items smaller than
+    // min_item_evals evaluations
+    const double target_items = std::max(
+        1.0, std::min(tuning.items_per_slot * slots, static_cast<double>(total_work) / std::max(1, tuning.min_item_evals)));
     const double work_per_item = std::max(1.0, static_cast<double>(total_work) / target_items);
     // features per item of each node
     std::vector<int> per(M);
@@ -846,6 +1122,69 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
     });
 }
 
+void split_items_into_chunks(const std::vector<int>& node_counts, int chunk, int n_chunks,
+                             std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
+                             std::vector<int>& chunk_begin) {
+    const int M = static_cast<int>(node_counts.size());
+    std::vector<EvalItem> out;
+    out.reserve(items.size() + static_cast<size_t>(M) * n_chunks);
+    range.assign(M + 1, 0);
+    int node = -1;
+    for (const EvalItem& it : items) {   // items are node-major
+        while (node < it.node) range[++node] = static_cast<int>(out.size());
+        for (int f = it.f_begin; f < it.f_end;) {
+            const int e = std::min(it.f_end, (f / chunk + 1) * chunk);
+            EvalItem p = it;
+            p.f_begin = f;
+            p.f_end = e;
+            out.push_back(p);
+            f = e;
+        }
+    }
+    while (node < M) range[++node] = static_cast<int>(out.size());
+    items.swap(out);
+    const int n = static_cast<int>(items.size());
+    order.resize(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const int cx = items[x].f_begin / chunk, cy = items[y].f_begin / chunk;
+        if (cx != cy) return cx < cy;
+        return static_cast<long long>(node_counts[items[x].node]) * (items[x].f_end - items[x].f_begin) >
+               static_cast<long long>(node_counts[items[y].node]) * (items[y].f_end - items[y].f_begin);
+    });
+    chunk_begin.assign(n_chunks + 1, n);
+    for (int q = n - 1; q >= 0; q--) chunk_begin[items[order[q]].f_begin / chunk] = q;
+    for (int c = n_chunks - 1; c >= 0; c--) chunk_begin[c] = std::min(chunk_begin[c], chunk_begin[c + 1]);
+}
+
+// Rows of the staged table node by node, and the pass-1 order of the rows (sorted by pixel).
+void LevelEvaluator::stage_order(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
+                                 int M, const std::vector<int>& node_counts, long long rows) {
+    h_row_base_.assign(M + 1, 0);
+    for (int n = 0; n < M; n++) h_row_base_[n + 1] = h_row_base_[n] + node_counts[n];
+    row_base_.reserve(M + 1);
+    row_pos_.reserve(rows);
+    image_key_.reserve(rows);
+    image_key_sorted_.reserve(rows);
+    row_ids_.reserve(rows);
+    frame_order_.reserve(rows);
+    CF_CUDA_CHECK(cudaMemcpyAsync(row_base_.get(), h_row_base_.data(), sizeof(long long) * (M + 1),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    launch(ctx, "stage_rows", dim3(static_cast<unsigned>((rows + 255) / 256)), dim3(256), 0, stage_rows_kernel,
+           nodes_dev, row_base_.get(), M, rows, samples, ds.width, ds.plane, row_pos_.get(), image_key_.get(),
+           row_ids_.get());
+    int end_bit = 1;
+    while (end_bit < 64 && (1ull << end_bit) < static_cast<unsigned long long>(ds.n) * ds.plane) end_bit++;
+    size_t temp = 0;
+    CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp, image_key_.get(), image_key_sorted_.get(),
+                                                  row_ids_.get(), frame_order_.get(), static_cast<int>(rows), 0,
+                                                  end_bit, ctx->stream));
+    sort_temp_.reserve(temp);
+    CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(sort_temp_.get(), temp, image_key_.get(), image_key_sorted_.get(),
+                                                  row_ids_.get(), frame_order_.get(), static_cast<int>(rows), 0,
+                                                  end_bit, ctx->stream));
+}
+
 // ------------------------------------------------------------------------------------------------
 void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
                               const uint32_t* node_hist_dev, int M, const std::vector<int>& node_counts, int C,
@@ -857,16 +1196,51 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     tuning = EvalTuning::of(ctx);
     const int slots = ctx->num_sms * tuning.ctas_per_sm;
     const bool sharded = shard.world > 1;
+    // staged bins: where the integral images do not fit in L2 and fewer than half the samples sit in
+    // nodes large enough to be cut into frame slices (those levels gather from L2 already, fused), or
+    // on every level with stage_bins = 2; the bins are bytes (T <= 255)
+    long long rows = 0, big_rows = 0;
+    for (int c : node_counts) {
+        rows += c;
+        if (c >= kChunkBigNodeSamples) big_rows += c;
+    }
+    const size_t frame_bytes = static_cast<size_t>(ds.n) * ds.plane * (3 * sizeof(float) + sizeof(int2));
+    const bool stage = tuning.stage_bins != 0 && !sharded && T <= 255 && rows > 0 && rows < INT_MAX &&
+                       (tuning.stage_bins == 2 || (frame_bytes > ctx->l2_bytes && 2 * big_rows < rows));
+    // the staged search reads bytes instead of gathering, so it needs no L1: a larger histogram and
+    // tiles of up to 32 features, and items of whole 32-feature rows (fewer, larger items: no CTAs
+    // need to share a node's gathers)
+    EvalTuning plan = tuning;
+    if (stage) {
+        plan.ft_max = kStagedFeatures;
+        plan.bins_budget_words = std::max(plan.bins_budget_words, kStagedBinsWords);
+        plan.feature_granule = kStageTile;
+        plan.items_per_slot = std::min(plan.items_per_slot, kStagedItemsPerSlot);
+    }
     int budget = 0;
-    level_eval_smem(C, T, tuning, &budget);
+    level_eval_smem(C, T, plan, &budget);
     // sample chunks of a node's items merge their counts on this device, so they are not sharded; a
     // chunked item covers at most the features of the smallest tile (all C classes present)
     const int chunk_features =
-        sharded ? 0 : tile_features(budget, C, T + 1, tuning.ft_max, tuning.sample_groups != 0);
+        sharded || stage ? 0 : tile_features(budget, C, T + 1, plan.ft_max, plan.sample_groups != 0);
     int n_groups = 0;
     const int max_groups = static_cast<int>(kMaxChunkGroupBytes / (sizeof(uint32_t) * static_cast<size_t>(budget)));
-    plan_level_items(node_counts, F, tuning, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups,
+    plan_level_items(node_counts, F, plan, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups,
                      max_groups);
+    int stage_chunk = 0, n_chunks = 0;
+    long long stage_stride = 0;
+    if (stage) {
+        // feature chunks of whole 32-feature tiles whose table fits stage_max_mb, as even as possible
+        const long long f_pad = (F + kStageTile - 1) / kStageTile * kStageTile;
+        const long long max_bytes = static_cast<long long>(tuning.stage_max_mb) << 20;
+        const long long tiles_max = std::max<long long>(1, max_bytes / rows / kStageTile);
+        n_chunks = static_cast<int>((f_pad / kStageTile + tiles_max - 1) / tiles_max);
+        stage_chunk = static_cast<int>((f_pad / kStageTile + n_chunks - 1) / n_chunks) * kStageTile;
+        n_chunks = (F + stage_chunk - 1) / stage_chunk;
+        stage_stride = stage_chunk;
+        split_items_into_chunks(node_counts, stage_chunk, n_chunks, h_items_, h_range_, h_order_, h_chunk_begin_);
+    }
+    last_stage_chunks = stage ? n_chunks : 0;
     const int n_items = static_cast<int>(h_items_.size());
     // this process's items: every position of the work order, or positions rank, rank + world, ...
     h_local_order_.clear();
@@ -914,14 +1288,49 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     args.n_items = n_local;
     args.queue = queue_.get();
     args.cands = cands_.get();
-    args.ft_max = tuning.ft_max;
+    args.ft_max = plan.ft_max;
     args.bins_budget = budget;
     args.group_bins = n_groups > 0 ? group_bins_.get() : nullptr;
     args.group_count = n_groups > 0 ? group_count_.get() : nullptr;
     args.dump_left = dump_left;
-    if (n_local > 0) launch_level_eval(ctx, args, std::min(n_local, slots), tuning);
+    node_consts_.reserve(sizeof(NodeConsts) * static_cast<size_t>(M));
+    args.node_consts = reinterpret_cast<const NodeConsts*>(node_consts_.get());
+    launch(ctx, "node_consts", dim3((M + 127) / 128), dim3(128), 0, node_consts_kernel, M, C, node_hist_dev,
+           reinterpret_cast<NodeConsts*>(node_consts_.get()));
+    if (stage) {
+        queue_.reserve(n_chunks);
+        CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int) * n_chunks, ctx->stream));
+        stage_order(ctx, ds, samples, nodes_dev, M, node_counts, rows);
+        stage_.reserve(static_cast<size_t>(rows) * stage_stride);
+        args.staged = stage_.get();
+        args.staged_stride = stage_stride;
+        args.row_base = row_base_.get();
+        StageArgs sa;
+        sa.ds = ds;
+        sa.samples = samples;
+        sa.frame_order = frame_order_.get();
+        sa.row_pos = row_pos_.get();
+        sa.rows = rows;
+        sa.packs = lf.packs.get();
+        sa.sorted_thr = lf.sorted_thr.get();
+        sa.T = T;
+        sa.stride = stage_stride;
+        sa.out = stage_.get();
+        for (int c = 0; c < n_chunks; c++) {
+            sa.f_first = c * stage_chunk;
+            sa.n_feat = std::min(stage_chunk, F - sa.f_first);
+            launch_stage_bins(ctx, sa);
+            args.staged_f0 = sa.f_first;
+            args.order = order_.get() + h_chunk_begin_[c];
+            args.n_items = h_chunk_begin_[c + 1] - h_chunk_begin_[c];
+            args.queue = queue_.get() + c;
+            if (args.n_items > 0) launch_level_eval(ctx, args, std::min(args.n_items, slots), plan);
+        }
+    } else if (n_local > 0) {
+        launch_level_eval(ctx, args, std::min(n_local, slots), plan);
+    }
     if (sharded) exchange(ctx, n_items);
-    launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F,
+    launch(ctx, "reduce_candidates", dim3((M + 7) / 8), dim3(256), 0, reduce_candidates_kernel, M, F,
            item_range_.get(), cands_.get(), lf.thr.get(), splits_dev);
 }
 
@@ -1264,7 +1673,7 @@ extern "C" cf_status cf_evaluate_best_splits_noalloc(cf_context* ctx, const floa
         args.group_count = nullptr;
         args.dump_left = nullptr;
         launch_level_eval(ctx, args, std::min(n_items, slots), tuning);
-        launch(ctx, "reduce_candidates", dim3((M + 127) / 128), dim3(128), 0, reduce_candidates_kernel, M, F, d_range,
+        launch(ctx, "reduce_candidates", dim3((M + 7) / 8), dim3(256), 0, reduce_candidates_kernel, M, F, d_range,
                d_cands, thresholds, best);
         CF_CUDA_CHECK(cudaStreamSynchronize(st));
     });

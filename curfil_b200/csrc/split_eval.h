@@ -49,9 +49,12 @@ struct EvalTuning {
     int bins_budget_words = 7168;   // shared-memory histogram budget per CTA (u32 words)
     int warp_aggregate = 1;       // __match_any_sync aggregation of the shared-memory increments
     int ctas_per_sm = 3;
-    double items_per_slot = 64.0; // work items per resident CTA for load balance
-    int feature_granule = 8;      // a work item covers a multiple of this many features
+    double items_per_slot = 2048.0; // work items per resident CTA at most
+    int feature_granule = 4;      // a work item covers a multiple of this many features
     int sample_groups = 0;        // 1: lanes take (sample, feature) pairs of consecutive samples
+    int min_item_evals = 16384;   // feature evaluations per work item at least
+    int stage_bins = 1;           // 0 never, 1 when the integral images exceed L2, 2 always (levels without slices)
+    int stage_max_mb = 8192;      // staged bin table size limit (MiB)
 
     static EvalTuning of(cf_context* ctx);
 };
@@ -76,6 +79,23 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
                       std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
                       int chunk_features = 0, int* n_groups = nullptr, int max_groups = 0);
 
+// Staged bins (levels without sliced nodes): pass 1 computes the threshold bin of every (sample,
+// feature) with the level's samples taken in frame order, so the resident CTAs gather from one or two
+// frames at a time (L2 hits), and writes it to a byte table [row][feature]; pass 2 is the split
+// search reading its bins from the table. Rows are the level's samples node by node; the table
+// holds at most stage_max_mb MiB, so a level whose table would be larger runs in feature chunks
+// (multiples of kStageTile features), each pass 1 followed by the items of its features.
+constexpr int kStageTile = 32;   // features per pass-1 work item
+// launch shape of the pass-2 search (level_eval reading staged bins)
+constexpr int kStagedFeatures = 32;           // features per tile at most
+constexpr int kStagedBinsWords = 12288;       // histogram words per CTA
+constexpr double kStagedItemsPerSlot = 64.0;  // work items per resident CTA at most
+// Splits every item at the chunk boundaries (multiples of `chunk` features) and orders the items
+// chunk by chunk, largest first within a chunk; chunk_begin[c] is the first order position of chunk c.
+void split_items_into_chunks(const std::vector<int>& node_counts, int chunk, int n_chunks,
+                             std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
+                             std::vector<int>& chunk_begin);
+
 class LevelEvaluator {
 public:
     // nodes_dev / node_hist_dev: M node descriptors and [M][C] histograms on the device;
@@ -85,6 +105,7 @@ public:
                   const LevelFeatures& lf, cf_split* splits_dev, uint32_t* dump_left = nullptr);
     EvalTuning tuning;            // the context's tuning at the last evaluate call
     int64_t last_items = 0;
+    int last_stage_chunks = 0;    // feature chunks of the staged bins at the last call (0: not staged)
     int64_t last_local_evals = 0; // feature evaluations this process ran at the last evaluate call
 
     // Sharding of a level's work items over `world` processes (each holding the same dataset,
@@ -99,6 +120,8 @@ public:
 
 private:
     void exchange(cf_context* ctx, int n_items);
+    void stage_order(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev, int M,
+                     const std::vector<int>& node_counts, long long rows);
     std::vector<ItemCandidates> h_cands_, h_send_, h_recv_;
     std::vector<int> h_local_order_;
     DevArray<EvalItem> items_;
@@ -108,6 +131,15 @@ private:
     DevArray<int> queue_;
     DevArray<uint32_t> group_bins_;   // [groups][bins budget] merged counts of chunked items
     DevArray<int> group_count_;       // [groups] chunks finished
+    DevArray<unsigned char> node_consts_;   // [M] scoring constants of each node
+    DevArray<uint8_t> stage_;         // [rows][stride] staged bins of one feature chunk
+    DevArray<long long> row_base_;    // [M + 1] first row of each node
+    DevArray<int> row_pos_;           // [rows] position of each row's sample in the level's array
+    DevArray<unsigned long long> image_key_, image_key_sorted_;   // pixel (frame, y, x) of each row
+    DevArray<int> row_ids_, frame_order_;   // rows, and rows in pixel order
+    DevArray<unsigned char> sort_temp_;
+    std::vector<long long> h_row_base_;
+    std::vector<int> h_chunk_begin_;
     std::vector<EvalItem> h_items_;
     std::vector<int> h_order_;
     std::vector<int> h_range_;

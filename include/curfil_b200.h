@@ -116,18 +116,30 @@ typedef struct cf_eval_tuning {
     int32_t bins_budget_words;   /* histogram words per CTA, 1024..49152 (default 7168) */
     int32_t warp_aggregate;      /* 1: warp-aggregated shared increments, 0: plain atomics (default) */
     int32_t ctas_per_sm;         /* resident CTAs per SM the kernel is compiled for, 1..4 (default 3) */
-    int32_t feature_granule;     /* work items cover a multiple of this many features, 1..64 (default 8) */
-    float items_per_slot;        /* work items per resident CTA, (0, 1024] (default 64) */
+    int32_t feature_granule;     /* work items cover a multiple of this many features, 1..64 (default 4) */
+    float items_per_slot;        /* work items per resident CTA at most, (0, 8192] (default 2048) */
     int32_t sample_groups;       /* 0: each thread takes one sample through the tile's features; 1 (default):
                                     the lanes of a warp take (sample, feature) pairs of a few consecutive
                                     samples (neighbours in the image, so gathers share L1 lines) */
+    int32_t min_item_evals;      /* feature evaluations per work item at least, 256..2^30 (default 16384): a
+                                    level gets items_per_slot items per resident CTA or as many as hold this
+                                    much work, whichever is fewer. Many items per node keep many CTAs on
+                                    the same samples at once (their gathers share L2), but small items
+                                    pay their setup more often */
+    int32_t stage_bins;          /* 1 (default): levels without sliced nodes whose integral images exceed the
+                                    L2 cache are searched in two passes: the threshold bins of every
+                                    (sample, feature) are computed in frame order (the gathers of one
+                                    frame's samples share L2) into a byte table, then histogrammed node
+                                    by node. 0: never; 2: on every level without sliced nodes */
+    int32_t stage_max_mb;        /* device memory of the staged bin table at most, 1..65536 MiB (default 8192);
+                                    a level whose table is larger runs in feature chunks */
 } cf_eval_tuning;
 cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out);
 cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning);
 /* Project-written autotuner (no reference counterpart): trains the given tree (as cf_train_tree,
  * level-batched) under candidate launch shapes, starting from the context's current one, by
  * coordinate descent over (sample_groups, warp_aggregate), bins_budget_words, items_per_slot,
- * feature_granule and features_per_tile,
+ * feature_granule, min_item_evals, stage_bins and features_per_tile,
  * timing the split search with the trainer's CUDA events (min over `repeats`). Every candidate must
  * yield the identical tree (else CF_ERR_STATE). The fastest shape is set on the context and returned
  * with its time; `start_ms` is the time of the starting shape, `trials` the shapes measured (either

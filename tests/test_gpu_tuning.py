@@ -15,11 +15,18 @@ TUNINGS = [
     {"sample_groups": 0},
     {"sample_groups": 0, "warp_aggregate": 1},
     {"ctas_per_sm": 4, "bins_budget_words": 4096},
-    {"bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1, "items_per_slot": 1000.0},
+    {"bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1, "items_per_slot": 1000.0,
+     "min_item_evals": 256},
+    {"items_per_slot": 8192.0, "min_item_evals": 256},
     {"sample_groups": 0, "bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1},
     {"ctas_per_sm": 1, "items_per_slot": 0.5, "feature_granule": 64, "features_per_tile": 64},
     {"sample_groups": 0, "ctas_per_sm": 1, "feature_granule": 64, "features_per_tile": 64},
     {"ctas_per_sm": 2, "bins_budget_words": 49152, "items_per_slot": 4.0, "feature_granule": 4},
+    {"stage_bins": 2},
+    {"stage_bins": 2, "warp_aggregate": 1, "stage_max_mb": 1},
+    {"stage_bins": 2, "sample_groups": 0, "bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1,
+     "stage_max_mb": 1},
+    {"stage_bins": 0},
 ]
 
 
@@ -43,7 +50,7 @@ def test_default_tuning_and_reset(ctx):
     ctx.set_tuning()
     d = ctx.get_tuning().as_dict()
     assert d["ctas_per_sm"] == 3 and d["warp_aggregate"] == 0 and d["features_per_tile"] == 16
-    assert d["sample_groups"] == 1
+    assert d["sample_groups"] == 1 and d["stage_bins"] == 1 and d["stage_max_mb"] == 8192
     ctx.set_tuning(items_per_slot=2.0)
     assert ctx.get_tuning().items_per_slot == 2.0
     ctx.set_tuning()
@@ -53,7 +60,8 @@ def test_default_tuning_and_reset(ctx):
 @pytest.mark.parametrize("bad", [{"ctas_per_sm": 0}, {"ctas_per_sm": 5}, {"features_per_tile": 1},
                                  {"features_per_tile": 65}, {"bins_budget_words": 100},
                                  {"bins_budget_words": 49153}, {"warp_aggregate": 2}, {"feature_granule": 0},
-                                 {"items_per_slot": 0.0}, {"items_per_slot": 2000.0}])
+                                 {"items_per_slot": 0.0}, {"items_per_slot": 9000.0}, {"min_item_evals": 100},
+                                 {"stage_bins": 3}, {"stage_max_mb": 0}])
 def test_invalid_tuning_rejected(ctx, bad):
     ctx.set_tuning()
     before = ctx.get_tuning().as_dict()

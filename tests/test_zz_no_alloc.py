@@ -117,7 +117,8 @@ def test_noalloc_many_work_items_halves_items_per_slot(setup):
     feats, thr = orc.generate_features(ods, s, 777, 16384, 2, 60, 15)
     old = ctx.get_tuning()
     try:
-        ctx.set_tuning(items_per_slot=1024.0)   # 40 nodes x 2048 items of 8 features: 81 920 items
+        # 40 nodes x ~2100 items of 4 features (84 000 items), more than the scratch's 65 536
+        ctx.set_tuning(items_per_slot=1024.0, min_item_evals=256)
         expected = cf.evaluate_best_splits(ds, offsets, s, C, feats, thr)
         lv = Level(ctx, ods, depth_pairs, offsets, s, feats, thr)
         for call in range(2):
