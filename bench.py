@@ -385,23 +385,31 @@ def headline(ctx, stream, local, rank, world, args, barrier, max_over_ranks, sum
     out["evals_per_step"] = total_evals / args.steps
     out["gpu_launches"] = int(launches)
     out["clocks"] = clocks.summary()
+    # the split search is level_eval (fused, or pass 2 reading staged bins) plus stage_bins (pass 1 of
+    # the staged levels); the roofline is that of the two together, with each kernel's share beside it
     eval_ms, eval_launches = ctx.kernel_time("level_eval")
-    out["kernel_ms"] = {k: ctx.kernel_time(k)[0] for k in ("level_eval", "gen_features", "sort_features",
-                                                            "route_flags", "route_scatter", "scan",
-                                                            "reduce_candidates")}
+    stage_ms, stage_launches = ctx.kernel_time("stage_bins")
+    out["kernel_ms"] = {k: ctx.kernel_time(k)[0] for k in ("level_eval", "stage_bins", "stage_rows", "node_consts",
+                                                            "gen_features", "sort_features", "route_flags",
+                                                            "route_scatter", "scan", "reduce_candidates")}
     bytes_per_eval = (BYTES_DEPTH_EVAL + BYTES_COLOR_EVAL) / 2.0
-    achieved = total_evals * bytes_per_eval / (eval_ms / 1e3) / 1e9 if eval_ms > 0 else None
+    search_ms = eval_ms + stage_ms
+    achieved = total_evals * bytes_per_eval / (search_ms / 1e3) / 1e9 if search_ms > 0 else None
     peak, peak_kind = load_peaks()
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "level_eval_traffic.txt")
+    tp = os.path.join(ROOT, "profiles", "split_search_traffic.txt")
     if os.path.exists(tp):
         for ln in open(tp):
             if ln.startswith("dram_bytes_per_feature_eval:"):
-                traffic = float(ln.split(":")[1]) * total_evals / max(1, eval_launches)
-    out["roofline"] = {"bound": "hbm", "kernel": "level_eval", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                       "frac": (achieved / peak) if achieved else None, "traffic": traffic, "peak_source": peak_kind,
-                       "bytes_per_eval": bytes_per_eval, "avg_launch_ms": eval_ms / max(1, eval_launches),
-                       "launches": eval_launches, "evals_per_launch": total_evals / max(1, eval_launches)}
+                traffic = float(ln.split(":")[1]) * total_evals / max(1, args.steps)
+    out["roofline"] = {"bound": "hbm", "kernel": "split search (level_eval + stage_bins)", "achieved": achieved,
+                       "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                       "traffic": traffic, "traffic_per": "step (one level)", "peak_source": peak_kind,
+                       "bytes_per_eval": bytes_per_eval, "ms_per_step": search_ms / max(1, args.steps),
+                       "kernels": {"level_eval": {"ms": eval_ms, "launches": eval_launches,
+                                                  "share": eval_ms / search_ms if search_ms else None},
+                                   "stage_bins": {"ms": stage_ms, "launches": stage_launches,
+                                                  "share": stage_ms / search_ms if search_ms else None}}}
     out["levels"] = [{"level": s.level, "nodes": s.num_nodes, "samples": s.num_samples,
                       "ms": statistics.median(per_level[s.level]) if per_level[s.level] else None,
                       "feature_evals_per_s": s.num_samples * C3["features"] / (statistics.median(per_level[s.level]) / 1e3)

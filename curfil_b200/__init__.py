@@ -68,7 +68,8 @@ class EvalTuning(ctypes.Structure):
                 ("warp_aggregate", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
                 ("feature_granule", ctypes.c_int32), ("items_per_slot", ctypes.c_float),
                 ("sample_groups", ctypes.c_int32), ("min_item_evals", ctypes.c_int32),
-                ("stage_bins", ctypes.c_int32), ("stage_max_mb", ctypes.c_int32)]
+                ("stage_bins", ctypes.c_int32), ("stage_max_mb", ctypes.c_int32),
+                ("sample_order", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

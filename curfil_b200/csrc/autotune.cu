@@ -132,6 +132,9 @@ extern "C" cf_status cf_autotune_split_search(cf_dataset* ds, int num_samples, c
                 cf_eval_tuning c = cur;
                 c.stage_bins = v;
                 consider(c);
+                c = cur;
+                c.sample_order = v;
+                consider(c);
             }
             for (int v : tiles) {
                 cf_eval_tuning c = cur;

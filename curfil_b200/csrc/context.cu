@@ -233,6 +233,7 @@ cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning) {
         CF_REQUIRE(t.stage_bins >= 0 && t.stage_bins <= 2, "cf_context_set_tuning: stage_bins must be 0, 1 or 2");
         CF_REQUIRE(t.stage_max_mb >= 1 && t.stage_max_mb <= 65536,
                    "cf_context_set_tuning: stage_max_mb must be in [1, 65536]");
+        CF_REQUIRE(t.sample_order >= 0 && t.sample_order <= 2, "cf_context_set_tuning: sample_order must be 0, 1 or 2");
         std::lock_guard<std::mutex> lock(ctx->mu);
         ctx->tuning = t;
     });

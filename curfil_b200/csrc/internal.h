@@ -156,7 +156,7 @@ struct cf_context {
     // sized for 16, not 32) left more L1 and were 3-12 % faster per level. Up to 2048 items per CTA
     // slot of at least 16 K evaluations, in multiples of 4 features, were 4-21 % faster on the levels
     // of that workload (more CTAs on one node's samples at a time, sharing their gathers in L2).
-    static cf_eval_tuning default_tuning() { return cf_eval_tuning{16, 7168, 0, 3, 4, 2048.0f, 1, 16384, 1, 8192}; }
+    static cf_eval_tuning default_tuning() { return cf_eval_tuning{16, 7168, 0, 3, 4, 2048.0f, 1, 16384, 1, 8192, 1}; }
     std::mutex mu;
     struct KernelEvents {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;

@@ -99,6 +99,10 @@ struct EvalArgs {
     long long staged_stride = 0;
     int staged_f0 = 0;
     const long long* row_base = nullptr;
+    const int* staged_flip_both = nullptr;   // nonzero: a sample of the level has flip 2
+    // fused search over a copy of the samples sorted by (node, frame, Morton code): node n's samples
+    // are rows row_base[n] .. of it; nullptr: the level's own array
+    const Sample* sorted_samples = nullptr;
     // per-node scoring constants computed once per level (node_consts_kernel); nullptr: every item
     // computes its node's constants itself
     const NodeConsts* node_consts = nullptr;
@@ -168,6 +172,57 @@ __device__ __noinline__ double score_from_cum(const uint32_t* cum, int stride, c
     return normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, hc)));
 }
 
+// score_from_cum with the work spread over a warp: the lanes evaluate the per-class terms (their
+// divisions and logarithms) and the three entropies in parallel, and every lane adds the terms in
+// score_from_cum's order, so the result is bit-identical (the serial form spends about 300 cycles
+// of dependent double arithmetic per class on one thread while its CTA waits). Called by all lanes.
+__device__ __noinline__ double score_from_cum_warp(const uint32_t* cum, int stride, const uint32_t* counts, int cp,
+                                                   double total, double hc, int lane) {
+    uint32_t L = 0;
+    for (int i = lane; i < cp; i += 32) L += cum[i * stride];
+    for (int off = 16; off > 0; off >>= 1) L += __shfl_xor_sync(kFull, L, off);
+    const double Ld = static_cast<double>(L);
+    const double Rd = __dsub_rn(total, Ld);
+    if (L == 0 || Rd == 0.0) return 0.0;
+    const double leftProb = __ddiv_rn(Ld, total);
+    const double rightProb = __ddiv_rn(Rd, total);
+    double e = 0.0;
+    if (lane == 1) e = entropy_of(Ld);
+    else if (lane == 2) e = entropy_of(Rd);
+    else if (lane == 3) e = entropy_of(total);
+    double ig = 0;
+    for (int base = 0; base < cp; base += 32) {
+        const int i = base + lane;
+        double tl = 0.0, tr = 0.0;
+        bool hl = false, hr = false;
+        if (i < cp) {
+            const uint32_t h = counts[i];
+            const uint32_t l = cum[i * stride];
+            const uint32_t r = h - l;
+            const double classProb = __ddiv_rn(static_cast<double>(h), total);
+            hl = l > 0;
+            hr = r > 0;
+            if (hl) tl = ig_term(static_cast<double>(l), total, leftProb, classProb);
+            if (hr) tr = ig_term(static_cast<double>(r), total, rightProb, classProb);
+        }
+        const unsigned bl = __ballot_sync(kFull, hl), br = __ballot_sync(kFull, hr);
+        const int m = min(32, cp - base);
+        for (int j = 0; j < m; j++) {
+            const double x = __shfl_sync(kFull, tl, j);
+            const double y = __shfl_sync(kFull, tr, j);
+            if ((bl >> j) & 1u) ig = __dadd_rn(ig, x);
+            if ((br >> j) & 1u) ig = __dadd_rn(ig, y);
+        }
+    }
+    ig = normalize_score(ig);   // the same value on every lane
+    if (ig == 0) return 0.0;
+    const double eL = __shfl_sync(kFull, e, 1), eR = __shfl_sync(kFull, e, 2), eT = __shfl_sync(kFull, e, 3);
+    const double hs = __ddiv_rn(__dsub_rn(__dadd_rn(eL, eR), eT), total);
+    return normalize_score(__ddiv_rn(__dmul_rn(2.0, ig), __dadd_rn(hs, hc)));
+}
+
+constexpr int kExactList = 256;   // pairs of a tile listed for the exact score (more: scored where found)
+
 template <bool kAgg, int kPad, int kMinBlocks, bool kGrouped>
 __global__ void __launch_bounds__(256, kMinBlocks)
 level_eval_kernel(EvalArgs a) {
@@ -183,6 +238,8 @@ level_eval_kernel(EvalArgs a) {
     __shared__ double s_best;
     __shared__ double s_cs[kMaxCand];
     __shared__ int s_ct[kMaxCand], s_cf[kMaxCand];
+    __shared__ int s_exact[kExactList];   // a tile's pairs needing the exact score
+    __shared__ int s_nexact;
     __shared__ double s_ns[kMaxCand];   // a tile's new candidates
     __shared__ int s_nt[kMaxCand], s_nf[kMaxCand];
     __shared__ int s_cn;
@@ -265,15 +322,20 @@ level_eval_kernel(EvalArgs a) {
         // the item's samples: the whole node, or one chunk of it
         const bool chunked = item.chunks > 1;
         const int N = chunked ? item.s_end - item.s_begin : nd.count;
-        const long long sbase = nd.start + (chunked ? item.s_begin : 0);
+        // the node's samples in the level's order, or in the Morton-sorted copy (rows node by node)
+        const Sample* const smps = a.sorted_samples ? a.sorted_samples : a.samples;
+        const long long sbase = (a.sorted_samples ? a.row_base[item.node] : nd.start) + (chunked ? item.s_begin : 0);
         const int ft = tile_features(a.bins_budget, cp, T1, a.ft_max, kGrouped);
 
         for (int f0 = item.f_begin; f0 < item.f_end; f0 += ft) {
             const int nf = min(ft, item.f_end - f0);
-            // ---- stage the tile
-            for (int i = tid; i < nf; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[f0 + i]);
+            // ---- stage the tile (the parameters and thresholds only where responses are computed: not
+            // for staged bins unless a sample of the level is evaluated both ways)
+            const bool need_thr = !a.staged || *a.staged_flip_both;
+            for (int i = tid; i < nf && need_thr; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[f0 + i]);
             const float* g_thr = a.sorted_thr + static_cast<long long>(f0) * T;
-            if (kPad) {
+            if (!need_thr) {
+            } else if (kPad) {
                 constexpr int kShift = kPad == 64 ? 6 : 5;
                 for (int i = tid; i < nf * kPad; i += blockDim.x) {
                     const int t = i & (kPad - 1);
@@ -377,7 +439,7 @@ level_eval_kernel(EvalArgs a) {
                         for (int u = 0; u < kUnroll; u++) {
                             const int s = s0 + js + u * step;
                             act[u] = fa && s < N;
-                            const Sample m = a.samples[sbase + min(s, N - 1)];
+                            const Sample m = smps[sbase + min(s, N - 1)];
                             px[u] = make_eval_pixel(a.ds, m);
                             row[u] = (fc * cp + s_lid[m.label]) * T1;
                             flip[u] = act[u] ? m.flip : 0;
@@ -402,7 +464,7 @@ level_eval_kernel(EvalArgs a) {
                     for (int s0 = warp * SPW; s0 < N; s0 += step) {
                         const int s = s0 + js;
                         const bool sv = s < N;
-                        const Sample smp = a.samples[sbase + min(s, N - 1)];
+                        const Sample smp = smps[sbase + min(s, N - 1)];
                         const EvalPixel px = make_eval_pixel(a.ds, smp);
                         const int lid = s_lid[smp.label];
                         const int flip = smp.flip;
@@ -427,7 +489,7 @@ level_eval_kernel(EvalArgs a) {
             // ---- histogram, sample-major over whole blocks of samples: each thread keeps one sample
             // and walks the tile's features, so the sample's neighbourhood is reused from L1
             for (int s0 = 0; s0 < n_major; s0 += nthr) {
-                const Sample smp = a.samples[sbase + s0 + tid];
+                const Sample smp = smps[sbase + s0 + tid];
                 const EvalPixel px = make_eval_pixel(a.ds, smp);
                 const int lid = s_lid[smp.label];
                 const int flip = smp.flip;
@@ -469,7 +531,7 @@ level_eval_kernel(EvalArgs a) {
             // all threads with a uniform trip count so warps stay converged
             const int Nt = a.staged ? 0 : N - n_major;
             if (!kGrouped && Nt > 0) {
-                const Sample* tail = a.samples + sbase + n_major;
+                const Sample* tail = smps + sbase + n_major;
                 const long long pairs = static_cast<long long>(nf) * Nt;
                 const int iters = static_cast<int>((pairs + nthr - 1) / nthr);
                 const int qstep = nthr / Nt;
@@ -579,19 +641,50 @@ level_eval_kernel(EvalArgs a) {
                 }
                 for (int off = 16; off > 0; off >>= 1) lbmax = fmaxf(lbmax, __shfl_xor_sync(kFull, lbmax, off));
                 if (lane == 0) s_wmax[warp] = lbmax;
+                if (tid == 0) s_nexact = 0;
                 __syncthreads();
                 float m = s_wmax[0];
                 for (int w = 1; w < static_cast<int>(blockDim.x >> 5); w++) m = fmaxf(m, s_wmax[w]);
                 const double floor_s = fmax(static_cast<double>(m), s_best) - 1e-13;
+                // pairs reaching the floor: scored where found (fused search: the scoring overlaps the
+                // other warps' gathers) or, reading staged bins, listed and scored after one barrier, a
+                // warp each if there are few (latency) or a thread each (throughput); the rest get -inf
+                const bool listed = a.staged != nullptr;
                 for (int i = tid; i < nf * T; i += blockDim.x) {
                     const float ub = s_bounds[i].y;
                     double sc = -INFINITY;
                     if (static_cast<double>(ub) >= floor_s) {
+                        const int k = listed ? atomicAdd(&s_nexact, 1) : kExactList;
+                        if (k < kExactList) {
+                            s_exact[k] = i;
+                            continue;
+                        }
                         const int fl = i / T;
                         const int t = i - fl * T;
                         sc = score_from_cum(s_bins + fl * cp * T1 + s_rank[fl * T + t], T1, s_counts, cp, total, hc);
                     }
                     s_scores[i] = sc;
+                }
+                if (listed) __syncthreads();
+                const int ne = listed ? min(s_nexact, kExactList) : 0;
+                const int nwarps = static_cast<int>(blockDim.x >> 5);
+                if (ne <= nwarps) {
+                    if (warp < ne) {
+                        const int i = s_exact[warp];
+                        const int fl = i / T;
+                        const int t = i - fl * T;
+                        const double sc = score_from_cum_warp(s_bins + fl * cp * T1 + s_rank[fl * T + t], T1, s_counts,
+                                                              cp, total, hc, lane);
+                        if (lane == 0) s_scores[i] = sc;
+                    }
+                } else {
+                    for (int k = tid; k < ne; k += blockDim.x) {
+                        const int i = s_exact[k];
+                        const int fl = i / T;
+                        const int t = i - fl * T;
+                        s_scores[i] =
+                            score_from_cum(s_bins + fl * cp * T1 + s_rank[fl * T + t], T1, s_counts, cp, total, hc);
+                    }
                 }
             }
             __syncthreads();
@@ -668,7 +761,9 @@ level_eval_kernel(EvalArgs a) {
                 }
                 __syncwarp();
             }
-            __syncthreads();
+            // no barrier here: the other warps stage the next tile while warp 0 merges the candidates
+            // (it reads only the scores and the candidate list, which the next tile writes after its
+            // first barrier)
         }
 
         if (tid == 0) {
@@ -687,15 +782,30 @@ level_eval_kernel(EvalArgs a) {
     }
 }
 
+// features per pass-1 work item: two tiles (64 features) were 1 % faster than one, the samples'
+// neighbourhoods serving more features while they are in L1
+constexpr int kStageItemFeatures = 2 * kStageTile;
+
+// bits 0..15 of v spread to the even bit positions (Morton order)
+__device__ __forceinline__ unsigned long long spread_bits(uint32_t v) {
+    unsigned long long x = v & 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0Full;
+    x = (x | (x << 2)) & 0x33333333ull;
+    x = (x | (x << 1)) & 0x55555555ull;
+    return x;
+}
+
 // ---- staged bins, pass 1 -------------------------------------------------------------------------
 // Rows of the staged table: row_base[n] + k is sample k of node n. stage_rows_kernel gives every row
-// its sample's position in the level's array and its pixel (frame, y, x) as the sort key of the pass-1
-// order: frame by frame, and within a frame in raster order, so neighbouring threads take samples
-// whose neighbourhoods overlap.
+// its sample's position in the level's array and its pixel as the sort key of the pass-1 order: frame
+// by frame, and within a frame in Morton (Z) order of (y, x), so the samples a CTA takes lie in a
+// compact patch and their neighbourhoods overlap in L1 (9 % faster than raster order, whose 256
+// samples span the frame's width).
 __global__ void stage_rows_kernel(const NodeDesc* __restrict__ nodes, const long long* __restrict__ row_base, int M,
-                                  long long rows, const Sample* __restrict__ samples, int W, long long plane,
+                                  long long rows, const Sample* __restrict__ samples, int node_shift,
                                   int* __restrict__ row_pos, unsigned long long* __restrict__ pixel_key,
-                                  int* __restrict__ row_ids) {
+                                  int* __restrict__ row_ids, int* __restrict__ flip_both) {
     const long long r = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (r >= rows) return;
     int lo = 0, hi = M - 1;   // the last node n with row_base[n] <= r
@@ -707,8 +817,17 @@ __global__ void stage_rows_kernel(const NodeDesc* __restrict__ nodes, const long
     const long long p = nodes[lo].start + (r - row_base[lo]);
     const Sample s = samples[p];
     row_pos[r] = static_cast<int>(p);
-    pixel_key[r] = static_cast<unsigned long long>(s.image) * plane + static_cast<long long>(s.y) * W + s.x;
+    pixel_key[r] = (static_cast<unsigned long long>(s.image) << 32) | (spread_bits(s.y) << 1) | spread_bits(s.x) |
+                   (node_shift > 0 ? static_cast<unsigned long long>(lo) << node_shift : 0ull);
     row_ids[r] = static_cast<int>(r);
+    if (s.flip == 2) *flip_both = 1;
+}
+
+// The Morton-sorted copy of a level's samples: out[k] is the sample of the k-th row in key order.
+__global__ void gather_sorted_samples_kernel(long long rows, const int* __restrict__ order, const int* __restrict__ row_pos,
+                                             const Sample* __restrict__ samples, Sample* __restrict__ out) {
+    const long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (k < rows) out[k] = samples[row_pos[order[k]]];
 }
 
 struct StageArgs {
@@ -721,7 +840,7 @@ struct StageArgs {
     const float* sorted_thr;  // [F][T]
     int T;
     int f_first, n_feat;      // this chunk's features [f_first, f_first + n_feat)
-    long long stride;         // row bytes, a multiple of kStageTile
+    long long stride;         // row bytes, a multiple of 32 (kStageTile)
     uint8_t* out;
 };
 
@@ -737,25 +856,28 @@ __global__ void __launch_bounds__(256, kStageCtasPerSm)
 stage_bins_kernel(StageArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     EvalFeat* s_params = reinterpret_cast<EvalFeat*>(smem);
-    float* s_thr = reinterpret_cast<float*>(smem + sizeof(EvalFeat) * kStageTile);
+    float* s_thr = reinterpret_cast<float*>(smem + sizeof(EvalFeat) * kStageItemFeatures);
     const int T = a.T;
     const int TP = kPad ? kPad : T;
+    // (rows padded against the two-way bank conflicts of the search, one word after every 32, were
+    // 2 % slower: the conflicts cost less than the extra index arithmetic)
+    const int TPS = TP;
     const int W = a.ds.width, H = a.ds.height;
-    const int tiles = (a.n_feat + kStageTile - 1) / kStageTile;
+    const int tiles = (a.n_feat + kStageItemFeatures - 1) / kStageItemFeatures;
     const long long blocks = (a.rows + 255) / 256;
     const long long n_items = blocks * tiles;
     for (long long q = blockIdx.x; q < n_items; q += gridDim.x) {
         const long long blk = q / tiles;
         const int j = static_cast<int>(q - blk * tiles);
-        const int fb = j * kStageTile;
-        const int nf = min(kStageTile, a.n_feat - fb);
+        const int fb = j * kStageItemFeatures;
+        const int nf = min(kStageItemFeatures, a.n_feat - fb);
         const int fg = a.f_first + fb;
         __syncthreads();   // the previous item's reads of the tile are done
         for (int i = threadIdx.x; i < nf; i += blockDim.x) s_params[i] = make_eval_feat(a.packs[fg + i]);
         const float* g_thr = a.sorted_thr + static_cast<long long>(fg) * T;
         for (int i = threadIdx.x; i < nf * TP; i += blockDim.x) {
             const int f = i / TP, t = i - f * TP;
-            s_thr[i] = t < T ? g_thr[f * T + t] : INFINITY;
+            s_thr[f * TPS + t] = t < T ? g_thr[f * T + t] : INFINITY;
         }
         __syncthreads();
         const long long r = blk * 256 + threadIdx.x;
@@ -767,9 +889,9 @@ stage_bins_kernel(StageArgs a) {
             uint32_t* dst = reinterpret_cast<uint32_t*>(a.out + static_cast<long long>(row) * a.stride + fb);
             uint32_t acc = 0;
             for (int f = 0; f < nf; f += 2) {
-                const int b0 = feature_bin(px, W, H, s_params[f], flip, SortedBins<kPad>{s_thr + f * TP, T});
+                const int b0 = feature_bin(px, W, H, s_params[f], flip, SortedBins<kPad>{s_thr + f * TPS, T});
                 const int b1 =
-                    f + 1 < nf ? feature_bin(px, W, H, s_params[f + 1], flip, SortedBins<kPad>{s_thr + (f + 1) * TP, T}) : 0;
+                    f + 1 < nf ? feature_bin(px, W, H, s_params[f + 1], flip, SortedBins<kPad>{s_thr + (f + 1) * TPS, T}) : 0;
                 acc |= static_cast<uint32_t>(b0 | (b1 << 8)) << (8 * (f & 3));
                 if ((f & 3) == 2 || f + 2 >= nf) {
                     dst[f >> 2] = acc;
@@ -988,9 +1110,9 @@ void launch_level_eval_a(cf_context* ctx, const EvalArgs& args, int grid, size_t
 template <int kPad>
 void launch_stage_bins_t(cf_context* ctx, const StageArgs& a) {
     const int TP = kPad ? kPad : a.T;
-    const size_t smem = sizeof(EvalFeat) * kStageTile + sizeof(float) * kStageTile * TP;
+    const size_t smem = sizeof(EvalFeat) * kStageItemFeatures + sizeof(float) * kStageItemFeatures * TP;
     set_level_eval_smem(stage_bins_kernel<kPad>, smem, kStageCtasPerSm);
-    const long long items = (a.rows + 255) / 256 * ((a.n_feat + kStageTile - 1) / kStageTile);
+    const long long items = (a.rows + 255) / 256 * ((a.n_feat + kStageItemFeatures - 1) / kStageItemFeatures);
     const int grid = static_cast<int>(std::min<long long>(items, static_cast<long long>(ctx->num_sms) * kStageCtasPerSm));
     launch(ctx, "stage_bins", dim3(grid), dim3(256), smem, stage_bins_kernel<kPad>, a);
 }
@@ -1035,6 +1157,7 @@ EvalTuning EvalTuning::of(cf_context* ctx) {
     e.min_item_evals = t.min_item_evals;
     e.stage_bins = t.stage_bins;
     e.stage_max_mb = t.stage_max_mb;
+    e.sample_order = t.sample_order;
     return e;
 }
 
@@ -1157,30 +1280,36 @@ void split_items_into_chunks(const std::vector<int>& node_counts, int chunk, int
     for (int c = n_chunks - 1; c >= 0; c--) chunk_begin[c] = std::min(chunk_begin[c], chunk_begin[c + 1]);
 }
 
-// Rows of the staged table node by node, and the pass-1 order of the rows (sorted by pixel).
+// Rows node by node, and their order sorted by (frame, Morton code), or with by_node by (node, frame,
+// Morton code) for the sorted sample copy of the fused search.
 void LevelEvaluator::stage_order(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev,
-                                 int M, const std::vector<int>& node_counts, long long rows) {
+                                 int M, const std::vector<int>& node_counts, long long rows, bool by_node) {
     h_row_base_.assign(M + 1, 0);
     for (int n = 0; n < M; n++) h_row_base_[n + 1] = h_row_base_[n] + node_counts[n];
     row_base_.reserve(M + 1);
     row_pos_.reserve(rows);
-    image_key_.reserve(rows);
-    image_key_sorted_.reserve(rows);
+    pixel_key_.reserve(rows);
+    pixel_key_sorted_.reserve(rows);
     row_ids_.reserve(rows);
     frame_order_.reserve(rows);
     CF_CUDA_CHECK(cudaMemcpyAsync(row_base_.get(), h_row_base_.data(), sizeof(long long) * (M + 1),
                                   cudaMemcpyHostToDevice, ctx->stream));
+    flip_both_.reserve(1);
+    CF_CUDA_CHECK(cudaMemsetAsync(flip_both_.get(), 0, sizeof(int), ctx->stream));
+    int end_bit = 33;   // 32 bits of Morton code, then the frame, then (by_node) the node
+    while (end_bit < 64 && (1ull << (end_bit - 32)) < static_cast<unsigned long long>(ds.n)) end_bit++;
+    const int node_shift = by_node ? end_bit : 0;
+    if (by_node)
+        while (end_bit < 64 && (1ull << (end_bit - node_shift)) < static_cast<unsigned long long>(M)) end_bit++;
     launch(ctx, "stage_rows", dim3(static_cast<unsigned>((rows + 255) / 256)), dim3(256), 0, stage_rows_kernel,
-           nodes_dev, row_base_.get(), M, rows, samples, ds.width, ds.plane, row_pos_.get(), image_key_.get(),
-           row_ids_.get());
-    int end_bit = 1;
-    while (end_bit < 64 && (1ull << end_bit) < static_cast<unsigned long long>(ds.n) * ds.plane) end_bit++;
+           nodes_dev, row_base_.get(), M, rows, samples, node_shift, row_pos_.get(), pixel_key_.get(), row_ids_.get(),
+           flip_both_.get());
     size_t temp = 0;
-    CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp, image_key_.get(), image_key_sorted_.get(),
+    CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp, pixel_key_.get(), pixel_key_sorted_.get(),
                                                   row_ids_.get(), frame_order_.get(), static_cast<int>(rows), 0,
                                                   end_bit, ctx->stream));
     sort_temp_.reserve(temp);
-    CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(sort_temp_.get(), temp, image_key_.get(), image_key_sorted_.get(),
+    CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(sort_temp_.get(), temp, pixel_key_.get(), pixel_key_sorted_.get(),
                                                   row_ids_.get(), frame_order_.get(), static_cast<int>(rows), 0,
                                                   end_bit, ctx->stream));
 }
@@ -1216,6 +1345,8 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
         plan.bins_budget_words = std::max(plan.bins_budget_words, kStagedBinsWords);
         plan.feature_granule = kStageTile;
         plan.items_per_slot = std::min(plan.items_per_slot, kStagedItemsPerSlot);
+        // (tiles kept at powers of two: the sample-group instance ran pass 2 in half the time of the
+        // one-sample-per-thread instance with unrounded tiles, 51 against 108 ms on a level of 128 nodes)
     }
     int budget = 0;
     level_eval_smem(C, T, plan, &budget);
@@ -1233,11 +1364,14 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
         // feature chunks of whole 32-feature tiles whose table fits stage_max_mb, as even as possible
         const long long f_pad = (F + kStageTile - 1) / kStageTile * kStageTile;
         const long long max_bytes = static_cast<long long>(tuning.stage_max_mb) << 20;
-        const long long tiles_max = std::max<long long>(1, max_bytes / rows / kStageTile);
+        const long long tiles_max = std::max<long long>(1, max_bytes / rows / kStageTile - 1);   // (- 1: the row pad)
         n_chunks = static_cast<int>((f_pad / kStageTile + tiles_max - 1) / tiles_max);
         stage_chunk = static_cast<int>((f_pad / kStageTile + n_chunks - 1) / n_chunks) * kStageTile;
         n_chunks = (F + stage_chunk - 1) / stage_chunk;
-        stage_stride = stage_chunk;
+        // rows an odd number of 32-byte sectors apart: with a power-of-two stride (1024 B for chunks of
+        // 1024 features) a node's rows fell into few L2 sets, and pass 2 read its segments 6-7 times
+        // from DRAM
+        stage_stride = stage_chunk / 32 % 2 == 0 ? stage_chunk + 32 : stage_chunk;
         split_items_into_chunks(node_counts, stage_chunk, n_chunks, h_items_, h_range_, h_order_, h_chunk_begin_);
     }
     last_stage_chunks = stage ? n_chunks : 0;
@@ -1300,11 +1434,12 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     if (stage) {
         queue_.reserve(n_chunks);
         CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int) * n_chunks, ctx->stream));
-        stage_order(ctx, ds, samples, nodes_dev, M, node_counts, rows);
+        stage_order(ctx, ds, samples, nodes_dev, M, node_counts, rows, false);
         stage_.reserve(static_cast<size_t>(rows) * stage_stride);
         args.staged = stage_.get();
         args.staged_stride = stage_stride;
         args.row_base = row_base_.get();
+        args.staged_flip_both = flip_both_.get();
         StageArgs sa;
         sa.ds = ds;
         sa.samples = samples;
@@ -1327,6 +1462,24 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
             if (args.n_items > 0) launch_level_eval(ctx, args, std::min(args.n_items, slots), plan);
         }
     } else if (n_local > 0) {
+        // one pass: where the frames exceed L2 (or sample_order = 2), a copy of the samples sorted by
+        // (node, frame, Morton code) puts each CTA's samples in a compact patch of the frame; counts
+        // do not depend on the order of a node's samples, and a slice of the sorted node still covers
+        // a run of frames
+        int key_bits = 32;
+        while ((1ll << (key_bits - 32)) < ds.n) key_bits++;
+        for (int m = M - 1; m > 0; m >>= 1) key_bits++;
+        const bool sorted = tuning.sample_order != 0 && rows > 0 && rows < INT_MAX && key_bits <= 64 &&
+                            (tuning.sample_order == 2 || frame_bytes > ctx->l2_bytes);
+        if (sorted) {
+            stage_order(ctx, ds, samples, nodes_dev, M, node_counts, rows, true);
+            sorted_samples_.reserve(rows);
+            launch(ctx, "gather_sorted_samples", dim3(static_cast<unsigned>((rows + 255) / 256)), dim3(256), 0,
+                   gather_sorted_samples_kernel, rows, frame_order_.get(), row_pos_.get(), samples,
+                   sorted_samples_.get());
+            args.sorted_samples = sorted_samples_.get();
+            args.row_base = row_base_.get();
+        }
         launch_level_eval(ctx, args, std::min(n_local, slots), plan);
     }
     if (sharded) exchange(ctx, n_items);

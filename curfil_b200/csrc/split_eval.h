@@ -55,6 +55,7 @@ struct EvalTuning {
     int min_item_evals = 16384;   // feature evaluations per work item at least
     int stage_bins = 1;           // 0 never, 1 when the integral images exceed L2, 2 always (levels without slices)
     int stage_max_mb = 8192;      // staged bin table size limit (MiB)
+    int sample_order = 1;         // 0 level order, 1 Morton-sorted copy when the frames exceed L2, 2 always
 
     static EvalTuning of(cf_context* ctx);
 };
@@ -121,7 +122,7 @@ public:
 private:
     void exchange(cf_context* ctx, int n_items);
     void stage_order(cf_context* ctx, const DsView& ds, const Sample* samples, const NodeDesc* nodes_dev, int M,
-                     const std::vector<int>& node_counts, long long rows);
+                     const std::vector<int>& node_counts, long long rows, bool by_node);
     std::vector<ItemCandidates> h_cands_, h_send_, h_recv_;
     std::vector<int> h_local_order_;
     DevArray<EvalItem> items_;
@@ -135,7 +136,9 @@ private:
     DevArray<uint8_t> stage_;         // [rows][stride] staged bins of one feature chunk
     DevArray<long long> row_base_;    // [M + 1] first row of each node
     DevArray<int> row_pos_;           // [rows] position of each row's sample in the level's array
-    DevArray<unsigned long long> image_key_, image_key_sorted_;   // pixel (frame, y, x) of each row
+    DevArray<int> flip_both_;         // set when a sample of the level has flip 2
+    DevArray<Sample> sorted_samples_; // [rows] the level's samples sorted by (node, frame, Morton code)
+    DevArray<unsigned long long> pixel_key_, pixel_key_sorted_;   // (frame, Morton code of y, x) of each row
     DevArray<int> row_ids_, frame_order_;   // rows, and rows in pixel order
     DevArray<unsigned char> sort_temp_;
     std::vector<long long> h_row_base_;

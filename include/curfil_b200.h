@@ -133,13 +133,17 @@ typedef struct cf_eval_tuning {
                                     by node. 0: never; 2: on every level without sliced nodes */
     int32_t stage_max_mb;        /* device memory of the staged bin table at most, 1..65536 MiB (default 8192);
                                     a level whose table is larger runs in feature chunks */
+    int32_t sample_order;        /* levels searched in one pass: 1 (default) reads a copy of the samples sorted
+                                    by (node, frame, Morton code of the pixel) where the integral images
+                                    exceed the L2 cache, so a CTA's samples lie in a compact patch and
+                                    share L1 lines; 0: the level's order; 2: always sorted */
 } cf_eval_tuning;
 cf_status cf_context_get_tuning(cf_context* ctx, cf_eval_tuning* out);
 cf_status cf_context_set_tuning(cf_context* ctx, const cf_eval_tuning* tuning);
 /* Project-written autotuner (no reference counterpart): trains the given tree (as cf_train_tree,
  * level-batched) under candidate launch shapes, starting from the context's current one, by
  * coordinate descent over (sample_groups, warp_aggregate), bins_budget_words, items_per_slot,
- * feature_granule, min_item_evals, stage_bins and features_per_tile,
+ * feature_granule, min_item_evals, stage_bins, sample_order and features_per_tile,
  * timing the split search with the trainer's CUDA events (min over `repeats`). Every candidate must
  * yield the identical tree (else CF_ERR_STATE). The fastest shape is set on the context and returned
  * with its time; `start_ms` is the time of the starting shape, `trials` the shapes measured (either

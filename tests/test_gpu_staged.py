@@ -30,6 +30,16 @@ def scene(ctx):
                 ds=cf.Dataset.from_raw(ctx, rgb, depth))
 
 
+def expected_chunks(rows, F, max_mb):
+    """Feature chunks of the staged table: whole 32-feature tiles, rows padded by one 32-byte sector,
+    at most max_mb MiB, as even as possible."""
+    tiles = -(-F // 32)
+    tiles_max = max(1, (max_mb << 20) // rows // 32 - 1)
+    n = -(-tiles // tiles_max)
+    chunk = -(-tiles // n) * 32
+    return -(-F // chunk)
+
+
 def staged_launches(ctx, fn):
     """Runs fn with kernel timing on; returns (fn's result, stage_bins launches)."""
     ctx.set_timing(True)
@@ -45,6 +55,7 @@ def staged_launches(ctx, fn):
 @pytest.mark.parametrize("T", [20, 32, 45, 100])
 @pytest.mark.parametrize("max_mb", [8192, 1])
 def test_staged_counts_equal_fused_and_oracle(ctx, scene, T, max_mb):
+    """Pass 1 + pass 2 (in one or several feature chunks) against the fused search and the oracle."""
     rng = np.random.default_rng(T + max_mb)
     # many nodes of ragged sizes, samples spread over all frames, flips 0 / 1 / 2
     sizes = [1, 2, 3, 900, 40, 257, 5, 1200, 64, 1, 333] + [int(x) for x in rng.integers(1, 120, 40)]
@@ -61,9 +72,7 @@ def test_staged_counts_equal_fused_and_oracle(ctx, scene, T, max_mb):
             ctx, lambda: cf.level_left_counts(scene["ds"], offsets, s, C, fe, th))
     finally:
         ctx.set_tuning()
-    rows = int(offsets[-1])
-    chunks = 1 if max_mb > 1 else -(-F // max(32, (1 << 20) // rows // 32 * 32))
-    assert launches == chunks and launches >= 1
+    assert launches == expected_chunks(int(offsets[-1]), F, max_mb) and launches >= 1
     np.testing.assert_array_equal(left2, left0)
     # (flags, which depend on how the items split the features, are not compared)
     for k in ("score", "feature", "threshold_index", "threshold"):
@@ -111,3 +120,28 @@ def test_staging_off_above_255_thresholds(ctx, scene):
     assert n == 0
     o = orc.histograms(scene["ods"], s[:300].view(orc.SAMPLE_DTYPE), fe, th, C, threads=4)
     np.testing.assert_array_equal(left[0], o[:, :, :, 0].transpose(1, 2, 0))
+
+
+def test_sorted_sample_copy_gives_the_same_counts(ctx, scene):
+    """The one-pass search over the copy sorted by (node, frame, Morton code) counts what the level's own
+    order counts, sliced nodes included."""
+    rng = np.random.default_rng(11)
+    sizes = [9000, 1, 17, 2500, 300] + [int(x) for x in rng.integers(1, 200, 30)]
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    s = H.random_samples(rng, N_IMG, W, HT, C, int(offsets[-1]), depth=scene["depth"], flips=True)
+    fe, th = orc.generate_features(scene["ods"], s, 21, 120, 24, 60, 15)
+    out = {}
+    try:
+        for order in (0, 2):
+            ctx.set_tuning(stage_bins=0, sample_order=order)
+            ctx.set_timing(True)
+            ctx.reset_timing()
+            out[order] = cf.level_left_counts(scene["ds"], offsets, s, C, fe, th)
+            assert (ctx.kernel_time("gather_sorted_samples")[1] > 0) == (order == 2)
+            ctx.set_timing(False)
+    finally:
+        ctx.set_timing(False)
+        ctx.set_tuning()
+    np.testing.assert_array_equal(out[2][1], out[0][1])
+    for k in ("score", "feature", "threshold_index", "threshold"):
+        np.testing.assert_array_equal(out[2][0][k], out[0][0][k], err_msg=k)

@@ -27,6 +27,9 @@ TUNINGS = [
     {"stage_bins": 2, "sample_groups": 0, "bins_budget_words": 1024, "features_per_tile": 2, "feature_granule": 1,
      "stage_max_mb": 1},
     {"stage_bins": 0},
+    {"stage_bins": 0, "sample_order": 2},
+    {"stage_bins": 0, "sample_order": 2, "sample_groups": 0, "warp_aggregate": 1},
+    {"stage_bins": 0, "sample_order": 0},
 ]
 
 
@@ -51,6 +54,7 @@ def test_default_tuning_and_reset(ctx):
     d = ctx.get_tuning().as_dict()
     assert d["ctas_per_sm"] == 3 and d["warp_aggregate"] == 0 and d["features_per_tile"] == 16
     assert d["sample_groups"] == 1 and d["stage_bins"] == 1 and d["stage_max_mb"] == 8192
+    assert d["sample_order"] == 1
     ctx.set_tuning(items_per_slot=2.0)
     assert ctx.get_tuning().items_per_slot == 2.0
     ctx.set_tuning()
@@ -61,7 +65,7 @@ def test_default_tuning_and_reset(ctx):
                                  {"features_per_tile": 65}, {"bins_budget_words": 100},
                                  {"bins_budget_words": 49153}, {"warp_aggregate": 2}, {"feature_granule": 0},
                                  {"items_per_slot": 0.0}, {"items_per_slot": 9000.0}, {"min_item_evals": 100},
-                                 {"stage_bins": 3}, {"stage_max_mb": 0}])
+                                 {"stage_bins": 3}, {"stage_max_mb": 0}, {"sample_order": 3}])
 def test_invalid_tuning_rejected(ctx, bad):
     ctx.set_tuning()
     before = ctx.get_tuning().as_dict()
