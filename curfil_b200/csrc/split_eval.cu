@@ -93,12 +93,15 @@ struct EvalArgs {
     uint32_t* group_bins;  // [groups][bins_budget] merged counts of chunked items, zero at launch
     int* group_count;      // [groups] chunks finished, zero at launch
     uint32_t* dump_left;   // optional [M][F][T][C] left counts (tests); nullptr in training
-    // staged bins: the bin of row r, feature f is staged[r * staged_stride + f - staged_f0]; the rows of
-    // node n start at row_base[n]. nullptr: the kernel computes its bins itself.
+    // staged bins: the bin of row r, feature f (g = f - staged_f0) is
+    // staged[((g / 32) * staged_rows + r) * 32 + g % 32]: 32-feature blocks, each [rows][32 bytes]; the
+    // rows of node n start at row_base[n], and row_label holds each row's label. nullptr: the kernel
+    // computes its bins itself.
     const uint8_t* staged = nullptr;
-    long long staged_stride = 0;
+    long long staged_rows = 0;
     int staged_f0 = 0;
     const long long* row_base = nullptr;
+    const uint8_t* row_label = nullptr;
     const int* staged_flip_both = nullptr;   // nonzero: a sample of the level has flip 2
     // fused search over a copy of the samples sorted by (node, frame, Morton code): node n's samples
     // are rows row_base[n] .. of it; nullptr: the level's own array
@@ -325,7 +328,8 @@ level_eval_kernel(EvalArgs a) {
         // the node's samples in the level's order, or in the Morton-sorted copy (rows node by node)
         const Sample* const smps = a.sorted_samples ? a.sorted_samples : a.samples;
         const long long sbase = (a.sorted_samples ? a.row_base[item.node] : nd.start) + (chunked ? item.s_begin : 0);
-        const int ft = tile_features(a.bins_budget, cp, T1, a.ft_max, kGrouped);
+        // (staged bins: a power of two <= 32 as well, so a tile never crosses a 32-feature block)
+        const int ft = tile_features(a.bins_budget, cp, T1, a.ft_max, kGrouped || a.staged);
 
         for (int f0 = item.f_begin; f0 < item.f_end; f0 += ft) {
             const int nf = min(ft, item.f_end - f0);
@@ -353,21 +357,24 @@ level_eval_kernel(EvalArgs a) {
             const int nthr = blockDim.x;
             const int n_major = kGrouped || a.staged ? 0 : (N / nthr) * nthr;
             if (a.staged) {
-                // ---- histogram of staged bins: the tile's bins of one sample are nw 4-byte words of its
-                // row (the segment starts `lead` bytes into the first); WL lanes (nw rounded up to a
-                // power of two) take one sample, a lane one word, i.e. four bins, and each lane
-                // kStagedUnroll samples per step so that many loads are in flight. A sample evaluated
-                // both ways (flip 2) has its unflipped bin staged; the flipped one is computed here by
-                // the sample's first lane.
-                const long long off = f0 - a.staged_f0;
-                const int lead = static_cast<int>(off & 3);
+                // ---- histogram of staged bins: the tile (a power of two of features, so within one
+                // 32-feature block) is, per sample, nw 4-byte words of the sample's 32-byte segment of
+                // the block (starting `lead` bytes into the first); the node's rows are consecutive
+                // segments, so a tile reads one contiguous run. WL lanes (nw rounded up to a power of
+                // two) take one sample, a lane one word, i.e. four bins, and each lane kStagedUnroll
+                // samples per step so that several loads are in flight. A sample evaluated both ways
+                // (flip 2) has its unflipped bin staged; the flipped one is computed here by the
+                // sample's first lane.
+                const int off = f0 - a.staged_f0;
+                const int o = off & 31;
+                const int lead = o & 3;
                 const int nw = (lead + nf + 3) >> 2;
                 const int WL = nw <= 1 ? 1 : 1 << (32 - __clz(nw - 1));
                 const int wi = lane & (WL - 1);
                 const int js = lane / WL;
                 const int step = static_cast<int>(blockDim.x >> 5) * (32 / WL);
-                const uint8_t* rows =
-                    a.staged + (a.row_base[item.node] + (sbase - nd.start)) * a.staged_stride + (off - lead);
+                const long long row0 = a.row_base[item.node] + (sbase - nd.start);
+                const uint8_t* rows = a.staged + ((static_cast<long long>(off >> 5) * a.staged_rows + row0) << 5) + (o - lead);
                 for (int s0 = warp * (32 / WL); s0 < N; s0 += kStagedUnroll * step) {   // trip count uniform in a warp
                     uint32_t v[kStagedUnroll];
                     int lid[kStagedUnroll], flip[kStagedUnroll];
@@ -378,16 +385,21 @@ level_eval_kernel(EvalArgs a) {
                         const int s = s0 + js + u * step;
                         const bool sv = s < N;
                         const int sc = sv ? s : N - 1;
-                        smp[u] = a.samples[sbase + sc];
                         act[u] = sv && wi < nw;
-                        v[u] = act[u] ? __ldg(reinterpret_cast<const uint32_t*>(rows + static_cast<long long>(sc) *
-                                                                                            a.staged_stride) + wi)
+                        v[u] = act[u] ? __ldg(reinterpret_cast<const uint32_t*>(rows + (static_cast<long long>(sc) << 5)) + wi)
                                       : 0u;
-                        flip[u] = sv && wi == 0 ? smp[u].flip : 0;
+                        if (need_thr) {   // a sample of the level has flip 2: the whole sample
+                            smp[u] = a.samples[sbase + sc];
+                            lid[u] = smp[u].label;
+                            flip[u] = sv && wi == 0 ? smp[u].flip : 0;
+                        } else {
+                            lid[u] = a.row_label[row0 + sc];
+                            flip[u] = 0;
+                        }
                     }
 #pragma unroll
                     for (int u = 0; u < kStagedUnroll; u++) {
-                        lid[u] = s_lid[smp[u].label];
+                        lid[u] = s_lid[lid[u]];
 #pragma unroll
                         for (int b = 0; b < 4; b++) {
                             const int f = 4 * wi + b - lead;
@@ -804,7 +816,7 @@ __device__ __forceinline__ unsigned long long spread_bits(uint32_t v) {
 // samples span the frame's width).
 __global__ void stage_rows_kernel(const NodeDesc* __restrict__ nodes, const long long* __restrict__ row_base, int M,
                                   long long rows, const Sample* __restrict__ samples, int node_shift,
-                                  int* __restrict__ row_pos, unsigned long long* __restrict__ pixel_key,
+                                  int* __restrict__ row_pos, uint8_t* __restrict__ row_label, unsigned long long* __restrict__ pixel_key,
                                   int* __restrict__ row_ids, int* __restrict__ flip_both) {
     const long long r = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (r >= rows) return;
@@ -817,6 +829,7 @@ __global__ void stage_rows_kernel(const NodeDesc* __restrict__ nodes, const long
     const long long p = nodes[lo].start + (r - row_base[lo]);
     const Sample s = samples[p];
     row_pos[r] = static_cast<int>(p);
+    row_label[r] = s.label;
     pixel_key[r] = (static_cast<unsigned long long>(s.image) << 32) | (spread_bits(s.y) << 1) | spread_bits(s.x) |
                    (node_shift > 0 ? static_cast<unsigned long long>(lo) << node_shift : 0ull);
     row_ids[r] = static_cast<int>(r);
@@ -840,8 +853,7 @@ struct StageArgs {
     const float* sorted_thr;  // [F][T]
     int T;
     int f_first, n_feat;      // this chunk's features [f_first, f_first + n_feat)
-    long long stride;         // row bytes, a multiple of 32 (kStageTile)
-    uint8_t* out;
+    uint8_t* out;             // [n_feat / 32 blocks][rows][32]
 };
 
 // One work item = 256 consecutive rows of the frame order x one tile of kStageTile features; items are
@@ -886,7 +898,7 @@ stage_bins_kernel(StageArgs a) {
             const Sample smp = a.samples[a.row_pos[row]];
             const EvalPixel px = make_eval_pixel(a.ds, smp);
             const bool flip = smp.flip == 1;
-            uint32_t* dst = reinterpret_cast<uint32_t*>(a.out + static_cast<long long>(row) * a.stride + fb);
+            uint8_t* seg = a.out + (static_cast<long long>(row) << 5);   // the row's segment of block 0
             uint32_t acc = 0;
             for (int f = 0; f < nf; f += 2) {
                 const int b0 = feature_bin(px, W, H, s_params[f], flip, SortedBins<kPad>{s_thr + f * TPS, T});
@@ -894,7 +906,8 @@ stage_bins_kernel(StageArgs a) {
                     f + 1 < nf ? feature_bin(px, W, H, s_params[f + 1], flip, SortedBins<kPad>{s_thr + (f + 1) * TPS, T}) : 0;
                 acc |= static_cast<uint32_t>(b0 | (b1 << 8)) << (8 * (f & 3));
                 if ((f & 3) == 2 || f + 2 >= nf) {
-                    dst[f >> 2] = acc;
+                    const int fw = fb + (f & ~3);   // first feature of the word
+                    *reinterpret_cast<uint32_t*>(seg + ((static_cast<long long>(fw >> 5) * a.rows) << 5) + (fw & 31)) = acc;
                     acc = 0;
                 }
             }
@@ -1288,6 +1301,7 @@ void LevelEvaluator::stage_order(cf_context* ctx, const DsView& ds, const Sample
     for (int n = 0; n < M; n++) h_row_base_[n + 1] = h_row_base_[n] + node_counts[n];
     row_base_.reserve(M + 1);
     row_pos_.reserve(rows);
+    row_label_.reserve(rows);
     pixel_key_.reserve(rows);
     pixel_key_sorted_.reserve(rows);
     row_ids_.reserve(rows);
@@ -1302,7 +1316,8 @@ void LevelEvaluator::stage_order(cf_context* ctx, const DsView& ds, const Sample
     if (by_node)
         while (end_bit < 64 && (1ull << (end_bit - node_shift)) < static_cast<unsigned long long>(M)) end_bit++;
     launch(ctx, "stage_rows", dim3(static_cast<unsigned>((rows + 255) / 256)), dim3(256), 0, stage_rows_kernel,
-           nodes_dev, row_base_.get(), M, rows, samples, node_shift, row_pos_.get(), pixel_key_.get(), row_ids_.get(),
+           nodes_dev, row_base_.get(), M, rows, samples, node_shift, row_pos_.get(), row_label_.get(), pixel_key_.get(),
+           row_ids_.get(),
            flip_both_.get());
     size_t temp = 0;
     CF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp, pixel_key_.get(), pixel_key_sorted_.get(),
@@ -1359,19 +1374,16 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     plan_level_items(node_counts, F, plan, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups,
                      max_groups);
     int stage_chunk = 0, n_chunks = 0;
-    long long stage_stride = 0;
+    size_t stage_bytes = 0;
     if (stage) {
         // feature chunks of whole 32-feature tiles whose table fits stage_max_mb, as even as possible
         const long long f_pad = (F + kStageTile - 1) / kStageTile * kStageTile;
         const long long max_bytes = static_cast<long long>(tuning.stage_max_mb) << 20;
-        const long long tiles_max = std::max<long long>(1, max_bytes / rows / kStageTile - 1);   // (- 1: the row pad)
+        const long long tiles_max = std::max<long long>(1, max_bytes / rows / kStageTile);
         n_chunks = static_cast<int>((f_pad / kStageTile + tiles_max - 1) / tiles_max);
         stage_chunk = static_cast<int>((f_pad / kStageTile + n_chunks - 1) / n_chunks) * kStageTile;
         n_chunks = (F + stage_chunk - 1) / stage_chunk;
-        // rows an odd number of 32-byte sectors apart: with a power-of-two stride (1024 B for chunks of
-        // 1024 features) a node's rows fell into few L2 sets, and pass 2 read its segments 6-7 times
-        // from DRAM
-        stage_stride = stage_chunk / 32 % 2 == 0 ? stage_chunk + 32 : stage_chunk;
+        stage_bytes = static_cast<size_t>(rows) * stage_chunk;
         split_items_into_chunks(node_counts, stage_chunk, n_chunks, h_items_, h_range_, h_order_, h_chunk_begin_);
     }
     last_stage_chunks = stage ? n_chunks : 0;
@@ -1435,9 +1447,10 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
         queue_.reserve(n_chunks);
         CF_CUDA_CHECK(cudaMemsetAsync(queue_.get(), 0, sizeof(int) * n_chunks, ctx->stream));
         stage_order(ctx, ds, samples, nodes_dev, M, node_counts, rows, false);
-        stage_.reserve(static_cast<size_t>(rows) * stage_stride);
+        stage_.reserve(stage_bytes);
         args.staged = stage_.get();
-        args.staged_stride = stage_stride;
+        args.staged_rows = rows;
+        args.row_label = row_label_.get();
         args.row_base = row_base_.get();
         args.staged_flip_both = flip_both_.get();
         StageArgs sa;
@@ -1449,7 +1462,6 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
         sa.packs = lf.packs.get();
         sa.sorted_thr = lf.sorted_thr.get();
         sa.T = T;
-        sa.stride = stage_stride;
         sa.out = stage_.get();
         for (int c = 0; c < n_chunks; c++) {
             sa.f_first = c * stage_chunk;

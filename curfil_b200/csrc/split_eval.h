@@ -80,17 +80,17 @@ void plan_level_items(const std::vector<int>& node_counts, int F, const EvalTuni
                       std::vector<EvalItem>& items, std::vector<int>& range, std::vector<int>& order,
                       int chunk_features = 0, int* n_groups = nullptr, int max_groups = 0);
 
-// Staged bins (levels without sliced nodes): pass 1 computes the threshold bin of every (sample,
-// feature) with the level's samples taken in frame order, so the resident CTAs gather from one or two
-// frames at a time (L2 hits), and writes it to a byte table [row][feature]; pass 2 is the split
-// search reading its bins from the table. Rows are the level's samples node by node; the table
-// holds at most stage_max_mb MiB, so a level whose table would be larger runs in feature chunks
-// (multiples of kStageTile features), each pass 1 followed by the items of its features.
-constexpr int kStageTile = 32;   // features per pass-1 work item
+// Staged bins (deep levels): pass 1 computes the threshold bin of every (sample, feature) with the
+// level's samples taken in frame and Morton order, so the resident CTAs gather from one or two frames
+// at a time (L2 hits), and writes it to a byte table of 32-feature blocks, each [row][32 bytes];
+// pass 2 is the split search reading its bins from the table. Rows are the level's samples node by
+// node; the table holds at most stage_max_mb MiB, so a level whose table would be larger runs in
+// feature chunks (multiples of kStageTile features), each pass 1 followed by the items of its features.
+constexpr int kStageTile = 32;   // features per table block
 // launch shape of the pass-2 search (level_eval reading staged bins)
 constexpr int kStagedFeatures = 32;           // features per tile at most
 constexpr int kStagedBinsWords = 12288;       // histogram words per CTA
-constexpr double kStagedItemsPerSlot = 64.0;  // work items per resident CTA at most
+constexpr double kStagedItemsPerSlot = 64.0;  // work items per resident CTA at most (16 and 256: the same)
 // Splits every item at the chunk boundaries (multiples of `chunk` features) and orders the items
 // chunk by chunk, largest first within a chunk; chunk_begin[c] is the first order position of chunk c.
 void split_items_into_chunks(const std::vector<int>& node_counts, int chunk, int n_chunks,
@@ -133,9 +133,10 @@ private:
     DevArray<uint32_t> group_bins_;   // [groups][bins budget] merged counts of chunked items
     DevArray<int> group_count_;       // [groups] chunks finished
     DevArray<unsigned char> node_consts_;   // [M] scoring constants of each node
-    DevArray<uint8_t> stage_;         // [rows][stride] staged bins of one feature chunk
+    DevArray<uint8_t> stage_;         // [blocks of 32 features][rows][32] staged bins of one feature chunk
     DevArray<long long> row_base_;    // [M + 1] first row of each node
     DevArray<int> row_pos_;           // [rows] position of each row's sample in the level's array
+    DevArray<uint8_t> row_label_;     // [rows] label of each row's sample
     DevArray<int> flip_both_;         // set when a sample of the level has flip 2
     DevArray<Sample> sorted_samples_; // [rows] the level's samples sorted by (node, frame, Morton code)
     DevArray<unsigned long long> pixel_key_, pixel_key_sorted_;   // (frame, Morton code of y, x) of each row

@@ -31,10 +31,10 @@ def scene(ctx):
 
 
 def expected_chunks(rows, F, max_mb):
-    """Feature chunks of the staged table: whole 32-feature tiles, rows padded by one 32-byte sector,
-    at most max_mb MiB, as even as possible."""
+    """Feature chunks of the staged table: whole 32-feature blocks, at most max_mb MiB, as even as
+    possible."""
     tiles = -(-F // 32)
-    tiles_max = max(1, (max_mb << 20) // rows // 32 - 1)
+    tiles_max = max(1, (max_mb << 20) // rows // 32)
     n = -(-tiles // tiles_max)
     chunk = -(-tiles // n) * 32
     return -(-F // chunk)
