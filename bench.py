@@ -370,7 +370,13 @@ def headline(ctx, stream, local, rank, world, args, barrier, max_over_ranks, sum
         start.record(stream)
         for i in range(args.steps):
             s = snaps[i % len(snaps)]
+            if i == args.profile_step:   # an Nsight Compute range (ncu --profile-from-start off)
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
             r = s.run()
+            if i == args.profile_step:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
             total_evals += r["evals"]
             per_level[s.level].append(r["ms"])
         end.record(stream)
@@ -900,6 +906,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="Poisson load per offered rate (0: skip)")
     ap.add_argument("--tuning", default="", help="split-search launch shape overrides, e.g. ctas_per_sm=4,"
                     "bins_budget_words=10240 (cf_eval_tuning field names)")
+    ap.add_argument("--profile-step", type=int, default=-1,
+                    help="bracket this timed headline step (0-based; steps cycle the levels) with a profiler range")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
