@@ -1340,17 +1340,13 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     tuning = EvalTuning::of(ctx);
     const int slots = ctx->num_sms * tuning.ctas_per_sm;
     const bool sharded = shard.world > 1;
-    // staged bins: where the integral images do not fit in L2 and fewer than half the samples sit in
-    // nodes large enough to be cut into frame slices (those levels gather from L2 already, fused), or
-    // on every level with stage_bins = 2; the bins are bytes (T <= 255)
-    long long rows = 0, big_rows = 0;
-    for (int c : node_counts) {
-        rows += c;
-        if (c >= kChunkBigNodeSamples) big_rows += c;
-    }
+    // staged bins: where the integral images do not fit in L2 (or on every level with stage_bins = 2);
+    // the bins are bytes (T <= 255)
+    long long rows = 0;
+    for (int c : node_counts) rows += c;
     const size_t frame_bytes = static_cast<size_t>(ds.n) * ds.plane * (3 * sizeof(float) + sizeof(int2));
     const bool stage = tuning.stage_bins != 0 && !sharded && T <= 255 && rows > 0 && rows < INT_MAX &&
-                       (tuning.stage_bins == 2 || (frame_bytes > ctx->l2_bytes && 2 * big_rows < rows));
+                       (tuning.stage_bins == 2 || frame_bytes > ctx->l2_bytes);
     // the staged search reads bytes instead of gathering, so it needs no L1: a larger histogram and
     // tiles of up to 32 features, and items of whole 32-feature rows (fewer, larger items: no CTAs
     // need to share a node's gathers)
@@ -1366,9 +1362,11 @@ void LevelEvaluator::evaluate(cf_context* ctx, const DsView& ds, const Sample* s
     int budget = 0;
     level_eval_smem(C, T, plan, &budget);
     // sample chunks of a node's items merge their counts on this device, so they are not sharded; a
-    // chunked item covers at most the features of the smallest tile (all C classes present)
+    // chunked item covers at most the features of the smallest tile (all C classes present). Staged
+    // levels chunk too: pass 2 of a level of one or two nodes has too few feature items to fill the
+    // GPU otherwise (its tiles are powers of two, so a chunked item stays inside a 32-feature block)
     const int chunk_features =
-        sharded || stage ? 0 : tile_features(budget, C, T + 1, plan.ft_max, plan.sample_groups != 0);
+        sharded ? 0 : tile_features(budget, C, T + 1, plan.ft_max, stage || plan.sample_groups != 0);
     int n_groups = 0;
     const int max_groups = static_cast<int>(kMaxChunkGroupBytes / (sizeof(uint32_t) * static_cast<size_t>(budget)));
     plan_level_items(node_counts, F, plan, slots, h_items_, h_range_, h_order_, chunk_features, &n_groups,
