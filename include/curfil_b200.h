@@ -126,11 +126,11 @@ typedef struct cf_eval_tuning {
                                     much work, whichever is fewer. Many items per node keep many CTAs on
                                     the same samples at once (their gathers share L2), but small items
                                     pay their setup more often */
-    int32_t stage_bins;          /* 1 (default): levels without sliced nodes whose integral images exceed the
-                                    L2 cache are searched in two passes: the threshold bins of every
-                                    (sample, feature) are computed in frame order (the gathers of one
-                                    frame's samples share L2) into a byte table, then histogrammed node
-                                    by node. 0: never; 2: on every level without sliced nodes */
+    int32_t stage_bins;          /* 1 (default): when the integral images exceed the L2 cache, every level
+                                    is searched in two passes: the threshold bins of every (sample,
+                                    feature) are computed in frame order (the gathers of one frame's
+                                    samples share L2) into a byte table, then histogrammed node by node
+                                    (huge nodes in sample slices). 0: never; 2: always (T <= 255) */
     int32_t stage_max_mb;        /* device memory of the staged bin table at most, 1..65536 MiB (default 8192);
                                     a level whose table is larger runs in feature chunks */
     int32_t sample_order;        /* levels searched in one pass: 1 (default) reads a copy of the samples sorted
