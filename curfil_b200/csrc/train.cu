@@ -11,6 +11,7 @@
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <thread>
 
 #include "host_rng.h"
 #include "route.h"
@@ -31,12 +32,77 @@ void validate_config(const cf_train_config* cfg) {
                "illegal configuration: maxImages must not be lower than imageCacheSize");
 }
 
+void check_sample(const cf_dataset* ds, const cf_sample& x, long long i, int C) {
+    CF_REQUIRE(x.image < static_cast<uint32_t>(ds->n), "sample " + std::to_string(i) + ": image index out of range");
+    CF_REQUIRE(x.x < ds->width && x.y < ds->height, "sample " + std::to_string(i) + ": pixel outside the image");
+    CF_REQUIRE(x.label < C, "sample " + std::to_string(i) + ": label >= number of classes");
+    CF_REQUIRE(x.flip <= 2, "sample " + std::to_string(i) + ": unknown flip setting");
+}
+
 void validate_samples(const cf_dataset* ds, const cf_sample* s, long long n, int C) {
-    for (long long i = 0; i < n; i++) {
-        CF_REQUIRE(s[i].image < static_cast<uint32_t>(ds->n), "sample " + std::to_string(i) + ": image index out of range");
-        CF_REQUIRE(s[i].x < ds->width && s[i].y < ds->height, "sample " + std::to_string(i) + ": pixel outside the image");
-        CF_REQUIRE(s[i].label < C, "sample " + std::to_string(i) + ": label >= number of classes");
-        CF_REQUIRE(s[i].flip <= 2, "sample " + std::to_string(i) + ": unknown flip setting");
+    for (long long i = 0; i < n; i++) check_sample(ds, s[i], i, C);
+}
+
+// validate_samples over host threads (the host-buffer entry points take millions of samples per
+// call), and with `hist` the class histogram [M][C] of the nodes whose samples are
+// [offsets[m], offsets[m + 1]) (a flip-2 sample counts twice). Each thread takes a contiguous range of
+// samples: nodes inside its range are its own rows of `hist`, the (at most two) nodes its range shares
+// with its neighbours are counted in private rows and added afterwards. On invalid input the error is
+// that of the first invalid sample, as validate_samples reports it.
+void scan_samples(const cf_dataset* ds, const cf_sample* s, long long n, int C, const int64_t* offsets, int M,
+                  uint32_t* hist) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = static_cast<int>(std::max<long long>(1, std::min<long long>(std::min<unsigned>(hw, 16u), n >> 18)));
+    if (T == 1 && !hist) {
+        validate_samples(ds, s, n, C);
+        return;
+    }
+    struct Part {
+        long long a = 0, b = 0, bad = -1;
+        int first = 0, last = 0;
+        std::vector<uint32_t> head, tail;
+    };
+    std::vector<Part> parts(T);
+    const uint32_t nimg = static_cast<uint32_t>(ds->n);
+    auto work = [&](Part& p) {
+        int node = 0;
+        if (hist) {
+            node = static_cast<int>(std::upper_bound(offsets, offsets + M + 1, static_cast<int64_t>(p.a)) - offsets) - 1;
+            p.first = node;
+            p.last = static_cast<int>(std::upper_bound(offsets, offsets + M + 1, static_cast<int64_t>(p.b - 1)) - offsets) - 1;
+            p.head.assign(C, 0);
+            if (p.last != p.first) p.tail.assign(C, 0);
+        }
+        for (long long i = p.a; i < p.b; i++) {
+            const cf_sample& x = s[i];
+            if (!(x.image < nimg && x.x < ds->width && x.y < ds->height && x.label < C && x.flip <= 2)) {
+                p.bad = i;
+                return;
+            }
+            if (!hist) continue;
+            while (offsets[node + 1] <= i) node++;
+            const uint32_t add = x.flip == 2 ? 2u : 1u;
+            if (node == p.first) p.head[x.label] += add;
+            else if (node == p.last) p.tail[x.label] += add;
+            else hist[static_cast<size_t>(node) * C + x.label] += add;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; t++) {
+        parts[t].a = n * t / T;
+        parts[t].b = n * (t + 1) / T;
+        if (t + 1 < T) pool.emplace_back(work, std::ref(parts[t]));
+    }
+    work(parts[T - 1]);
+    for (std::thread& th : pool) th.join();
+    for (const Part& p : parts)   // in sample order: the first invalid sample's error
+        if (p.bad >= 0) check_sample(ds, s[p.bad], p.bad, C);
+    if (!hist) return;
+    for (const Part& p : parts) {
+        if (p.a >= p.b) continue;
+        for (int c = 0; c < C; c++) hist[static_cast<size_t>(p.first) * C + c] += p.head[c];
+        if (p.last != p.first)
+            for (int c = 0; c < C; c++) hist[static_cast<size_t>(p.last) * C + c] += p.tail[c];
     }
 }
 
@@ -534,10 +600,10 @@ cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample*
         CF_REQUIRE(num_samples > 0 && num_features > 0 && num_thresholds > 0, "cf_generate_features: empty input");
         cf_context* ctx = ds->ctx;
         make_current(ctx);
-        validate_samples(ds, samples, num_samples, 256);
         TreeTrainer* tr = acquire_trainer(ds, 1, cf_train_config{}, CF_TRAIN_LEVEL_BATCHED);
         TreeTrainer::HostCall& hc = tr->host_;
-        upload_samples(ctx, hc.samples, samples, num_samples);
+        upload_samples(ctx, hc.samples, samples, num_samples);   // overlaps the check below
+        scan_samples(ds, samples, num_samples, 256, nullptr, 0, nullptr);
         LevelFeatures& lf = hc.lf;
         lf.reserve(num_features, num_thresholds);
         generate_level_features(ctx, view_of(ds), hc.samples.get(), static_cast<uint32_t>(num_samples), seed, box_radius,
@@ -567,21 +633,22 @@ void evaluate_level_host(cf_dataset* ds, int num_nodes, const int64_t* node_offs
         make_current(ctx);
         const long long n = node_offsets[num_nodes];
         CF_REQUIRE(node_offsets[0] == 0 && n > 0, "cf_evaluate_best_splits: node offsets must start at 0");
-        validate_samples(ds, samples, n, num_classes);
-        validate_thresholds(thresholds, static_cast<long long>(num_features) * num_thresholds);
         std::vector<NodeDesc> nodes(num_nodes);
         std::vector<int> counts(num_nodes);
-        std::vector<uint32_t> hist(static_cast<size_t>(num_nodes) * num_classes, 0);
         for (int i = 0; i < num_nodes; i++) {
             CF_REQUIRE(node_offsets[i + 1] > node_offsets[i], "cf_evaluate_best_splits: every node needs samples");
+            CF_REQUIRE(node_offsets[i + 1] - node_offsets[i] < (1LL << 31), "cf_evaluate_best_splits: node too large");
             nodes[i] = NodeDesc{node_offsets[i], static_cast<int>(node_offsets[i + 1] - node_offsets[i]), i};
             counts[i] = nodes[i].count;
-            for (long long s = node_offsets[i]; s < node_offsets[i + 1]; s++)
-                hist[static_cast<size_t>(i) * num_classes + samples[s].label] += samples[s].flip == 2 ? 2 : 1;
         }
         TreeTrainer* tr = acquire_trainer(ds, num_classes, cf_train_config{}, CF_TRAIN_LEVEL_BATCHED);
         TreeTrainer::HostCall& hc = tr->host_;
+        // the copy runs while the host checks the samples and counts the node histograms; nothing reads
+        // the copy before they pass
         upload_samples(ctx, hc.samples, samples, n);
+        std::vector<uint32_t> hist(static_cast<size_t>(num_nodes) * num_classes, 0);
+        scan_samples(ds, samples, n, num_classes, node_offsets, num_nodes, hist.data());
+        validate_thresholds(thresholds, static_cast<long long>(num_features) * num_thresholds);
         DevArray<NodeDesc>& d_nodes = hc.nodes;
         DevArray<uint32_t>& d_hist = hc.hist;
         DevArray<cf_split>& d_best = hc.best;

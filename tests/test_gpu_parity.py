@@ -479,3 +479,34 @@ def test_forest_train_end_to_end_matches_oracle(ctx):
         o = H.oracle_tree_dict(ot)
         H.compare_trees(g, o)
         np.testing.assert_array_equal(tree.prior(), np.bincount(labels.ravel(), minlength=6))
+
+
+def test_host_entry_point_large_level_matches_oracle(ctx, scene):
+    """cf_evaluate_best_splits on 600 000 host samples: the entry point checks the samples and counts
+    the node histograms on several host threads (ranges that split nodes between threads), and the
+    splits are the oracle's; an invalid sample is reported by its index, the first one when several are
+    invalid."""
+    rng = np.random.default_rng(600)
+    sizes = [290001, 1, 7, 210000, 99991]
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    s = H.random_samples(rng, 4, 96, 72, 40, int(offsets[-1]), depth=scene["depth"], flips=True)
+    for i in range(len(sizes)):
+        s["label"][offsets[i]:offsets[i + 1]] = rng.integers(0, 3 + 9 * i, sizes[i]) % 40
+    fe, th = orc.generate_features(scene["ods"], s[:20000], 61, 8, 5, 60, 15)
+    got = cf.evaluate_best_splits(scene["ds"], offsets, s, 40, fe, th)
+    for i in range(len(sizes)):
+        sl = s[offsets[i]:offsets[i + 1]]
+        node_hist = np.zeros(40, np.uint32)
+        np.add.at(node_hist, sl["label"], np.where(sl["flip"] == 2, 2, 1).astype(np.uint32))
+        sc = orc.scores(orc.histograms(scene["ods"], sl.view(orc.SAMPLE_DTYPE), fe, th, 40, threads=8), node_hist)
+        bf, bt, bs = orc.best_split(sc)
+        mine = sc[got["threshold_index"][i], got["feature"][i]]
+        if (got["feature"][i], got["threshold_index"][i]) != (bf, bt):
+            assert abs(mine - bs) <= 1e-6 * abs(bs), i
+        assert got["score"][i] == pytest.approx(mine, rel=1e-12, abs=1e-15), i
+    bad = s.copy()
+    bad["label"][450000] = 40
+    bad["x"][123456] = 96
+    with pytest.raises(cf.CurfilError) as e:
+        cf.evaluate_best_splits(scene["ds"], offsets, bad, 40, fe, th)
+    assert "sample 123456: pixel outside" in str(e.value), str(e.value)
