@@ -227,7 +227,10 @@ cf_status cf_generate_features(cf_dataset* ds, int num_samples, const cf_sample*
                                int num_features, int num_thresholds, int box_radius, int region_size,
                                int use_depth_images, int8_t* features, float* thresholds);
 /* evaluateBestSplits (random_tree_image.cpp:239-502) for all open nodes of one level in one
- * persistent launch. Node n owns samples [node_offsets[n], node_offsets[n+1]). */
+ * persistent launch. Node n owns samples [node_offsets[n], node_offsets[n+1]). The samples are
+ * checked (image, pixel, label, flip) and the node histograms counted on up to 16 host threads while
+ * the samples upload; an invalid sample fails the call with the index of the first one (as does
+ * cf_generate_features, which checks its samples the same way). */
 cf_status cf_evaluate_best_splits(cf_dataset* ds, int num_nodes, const int64_t* node_offsets,
                                   const cf_sample* samples, int num_classes, int num_features,
                                   int num_thresholds, const int8_t* features, const float* thresholds,
